@@ -1,0 +1,184 @@
+/*
+ * admp_b200 -- C ABI of the B200 (sm_100a) electrostatics hot path that sits
+ * behind torch-admp's CoulombForceModule / QEqForceModule / TorchNeighborList.
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer owned by the caller, except the
+ *    arguments documented as "host".  `stream` is a cudaStream_t (void* here so
+ *    this header needs no CUDA include).  Work is stream-ordered; entry points
+ *    that must return a size to the host (the neighbour-list count and the QEq
+ *    solver's convergence result) synchronise that stream.
+ *  - `dtype` selects the element type of the floating-point arrays:
+ *    ADMP_F64 (double) or ADMP_F32 (float).  Energies, virial-type reductions
+ *    and the CG dot products are always double.
+ *  - Gradient outputs ACCUMULATE (+=) into caller-zeroed buffers; NULL skips
+ *    that output.  Energies accumulate into double buffers.
+ *  - Index arrays (`pairs`) are int64 as produced by the reference
+ *    (row-major [npairs, 2]).
+ *  - Errors are never raised on the device: kernels record the first bad
+ *    index / non-finite value in an error word that the entry point reads
+ *    back, and return a status code.  admp_last_error_message() describes it.
+ *  - Scratch memory is passed in by the caller (`workspace`); the
+ *    *_workspace_size() queries give the bytes needed.  No entry point
+ *    allocates device memory.
+ */
+#ifndef ADMP_B200_H_
+#define ADMP_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ADMP_ABI_VERSION 1
+
+/* status codes */
+#define ADMP_OK 0
+#define ADMP_ERR_BAD_ARG 1           /* shape / argument error (ValueError in the reference) */
+#define ADMP_ERR_CUTOFF_TOO_LARGE 2  /* nblist.py:620-660 check_cutoff */
+#define ADMP_ERR_NOT_CONVERGED 3     /* CG hit max_iter (qeq.py:1261-1262 "did not converge") */
+#define ADMP_ERR_WORKSPACE 4         /* workspace too small */
+#define ADMP_ERR_CUDA 5              /* CUDA runtime error */
+#define ADMP_ERR_BAD_INDEX 6         /* pair index outside [0, natoms) */
+#define ADMP_ERR_CAPACITY 7          /* output capacity too small */
+#define ADMP_ERR_NONFINITE 8         /* NaN/Inf in positions or box */
+#define ADMP_ERR_MESH 9              /* unsupported mesh size */
+
+/* dtype codes */
+#define ADMP_F64 0
+#define ADMP_F32 1
+
+/* pair-term modes for admp_pair_energy */
+#define ADMP_PAIR_EWALD 0    /* erfc(kappa r) q_i q_j / r          pme.py:312-349 */
+#define ADMP_PAIR_OBC 1      /* q_i q_j / r, safe_inverse 1e-8     pme.py:529-561 */
+#define ADMP_PAIR_DAMPING 2  /* -erfc(r / 2 eta_ij) q_i q_j / r    qeq.py:60-129  */
+
+/* flags for admp_atom_terms */
+#define ADMP_TERM_SELF 1          /* pme.py:448-461 */
+#define ADMP_TERM_NON_NEUTRAL 2   /* pme.py:463-493 */
+#define ADMP_TERM_SLAB 4          /* pme.py:495-527 (axis in bits 8..9) */
+#define ADMP_TERM_DAMP_SELF 8     /* qeq.py:121-126 */
+#define ADMP_TERM_SITE 16         /* qeq.py:159-209 */
+
+int admp_abi_version(void);
+const char* admp_status_string(int status);
+/* Human-readable detail of the last non-OK status on this host thread. */
+const char* admp_last_error_message(void);
+/* Synchronous device-error checks (default on): entry points that launch
+ * kernels with index checks synchronise `stream` and report a bad index as a
+ * status.  With checks off, errors stay recorded on the device until
+ * admp_check_errors() (which always synchronises) reads and clears them. */
+void admp_set_sync_checks(int on);
+int admp_check_errors(void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Reciprocal-space PME.                                                     */
+/* Replaces CoulombForceModule._forward_pbc_reciprocal (pme.py:351-446) with  */
+/* recip.spread_charges / setup_kpts / _coeff_k_1 (recip.py:216-308,          */
+/* pme.py:661-683) and the autograd backward through them (utils.py:85-112). */
+/* nframes systems of `natoms` each; kmesh is HOST [nframes*3].               */
+/* Outputs per frame: energy (+=), dE/dpos [nf,N,3], dE/dq [nf,N],            */
+/* dE/dbox [nf,3,3] (all optional, accumulated).                              */
+/* ------------------------------------------------------------------------ */
+size_t admp_pme_recip_workspace_size(int dtype, int nframes, const int* kmesh);
+int admp_pme_recip(int dtype, int nframes, int natoms, const int* kmesh, const void* pos,
+                   const void* box, const void* q, double kappa, double ke, double* energy,
+                   void* dE_dpos, void* dE_dq, void* dE_dbox, void* workspace,
+                   size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Pair terms over a caller pair list.                                       */
+/* Replaces _forward_pbc_real (pme.py:312-349), _forward_obc (pme.py:529-561) */
+/* and the pair part of GaussianDampingForceModule (qeq.py:104-119).          */
+/* pairs [nf,P,2] int64, ds [nf,P], buffer_scales [nf,P] (dtype), q [nf,N],   */
+/* eta [nf,N] (damping only).  Outputs (all accumulated): energy [nf],       */
+/* dE/dds [nf,P], dE/dq [nf,N], dE/deta [nf,N].                               */
+/* ------------------------------------------------------------------------ */
+int admp_pair_energy(int dtype, int mode, int nframes, int natoms, long long npairs,
+                     const long long* pairs, const void* ds, const void* buffer_scales,
+                     const void* q, const void* eta, double kappa, double ke, double* energy,
+                     void* dE_dds, void* dE_dq, void* dE_deta, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Per-atom terms: Ewald self (pme.py:448-461), non-neutral correction        */
+/* (pme.py:463-493), slab correction (pme.py:495-527), damping self energy    */
+/* (qeq.py:121-126) and site energy chi q + hardness q^2 (qeq.py:159-209).    */
+/* `terms` (optional) receives [nf][5] = self, non_neutral, slab, damp_self,  */
+/* site.  pos/box are needed for SLAB / NON_NEUTRAL, eta for DAMP_SELF,       */
+/* chi/hardness for SITE.  Gradients accumulate.                              */
+/* ------------------------------------------------------------------------ */
+int admp_atom_terms(int dtype, int flags, int nframes, int natoms, const void* pos, const void* box,
+                    const void* q, const void* eta, const void* chi, const void* hardness,
+                    double kappa, double ke, double* energy, double* terms, void* dE_dq,
+                    void* dE_dpos, void* dE_dbox, void* dE_deta, void* dE_dchi, void* dE_dhard,
+                    void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Pair distances ds = |pbc_shift(r_i - r_j)| (nblist.py:517-551,            */
+/* spatial.py:15-36) or |r_j - r_i| without a box (pbc = 0), and their       */
+/* backward (gradient of a loss w.r.t. positions and box given dL/dds).       */
+/* ------------------------------------------------------------------------ */
+int admp_pair_distances(int dtype, int pbc, int natoms, long long npairs, const long long* pairs,
+                        const void* pos, const void* box, void* ds, void* stream);
+int admp_pair_distances_backward(int dtype, int pbc, int natoms, long long npairs,
+                                 const long long* pairs, const void* pos, const void* box,
+                                 const void* grad_ds, void* grad_pos, void* grad_box, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Cell-list neighbour list: TorchNeighborList.forward (nblist.py:304-445,   */
+/* 472-490) incl. check_cutoff (nblist.py:620-660).  Full list (both         */
+/* orders), 0.01 < r < rc with a box, r < rc without.  Two phases:            */
+/*   admp_nblist_count  -> *npairs (host), synchronises `stream`;            */
+/*   admp_nblist_fill   -> pairs [npairs,2] int64 sorted by (i, j) and        */
+/*                         buffer_scales [npairs] int64 (1 if i < j).         */
+/* The same workspace must be passed to both calls.                           */
+/* ------------------------------------------------------------------------ */
+size_t admp_nblist_workspace_size(int natoms);
+int admp_nblist_count(int dtype, int pbc, int natoms, const void* pos, const void* box,
+                      double cutoff, void* workspace, size_t workspace_bytes, long long* npairs,
+                      void* stream);
+int admp_nblist_fill(int dtype, int pbc, int natoms, const void* pos, const void* box,
+                     double cutoff, void* workspace, size_t workspace_bytes, long long* pairs,
+                     long long* buffer_scales, long long capacity, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Matrix-free projected CG solve of the QEq charges: replaces               */
+/* pgrad_optimize / QEqForceModule.solve_pgrad (qeq.py:609-712, 1117-1270)   */
+/* and the quadratic / LBFGS minimisers (qeq.py:1273-1527).  Minimises       */
+/* E(q) = site + Coulomb(PME) + damping subject to C q = b with linear CG    */
+/* (E is quadratic in q); stops when ||P grad||_2 / N < tol (qeq.py:1516).   */
+/*   flags: ADMP_QEQ_* below; kmesh HOST [3]; C [n_const, N] dtype;           */
+/*   b HOST [n_const] (double); q in: initial guess, out: solution.           */
+/*   rhs_shift: optional [N] added to chi (electrode potential b-vector).     */
+/* Returns ADMP_ERR_NOT_CONVERGED (q still written) when max_iter is hit.    */
+/* ------------------------------------------------------------------------ */
+#define ADMP_QEQ_KSPACE 1
+#define ADMP_QEQ_RSPACE 2
+#define ADMP_QEQ_DAMPING 4
+#define ADMP_QEQ_SLAB 8         /* slab axis in bits 8..9 */
+#define ADMP_QEQ_PROJECT_Q0 16  /* project the initial guess onto C q = b first */
+size_t admp_qeq_workspace_size(int dtype, int natoms, long long npairs, const int* kmesh,
+                               int n_const);
+int admp_qeq_solve(int dtype, int flags, int natoms, const int* kmesh, const void* pos,
+                   const void* box, long long npairs, const long long* pairs, const void* ds,
+                   const void* buffer_scales, const void* chi, const void* hardness,
+                   const void* eta, const void* rhs_shift, double kappa, double ke, int n_const,
+                   const void* C, const double* b, void* q, double tol, int max_iter,
+                   int* iters, double* resid, void* workspace, size_t workspace_bytes,
+                   void* stream);
+
+/* Hessian-vector product of the same quadratic form (dE/dq at p minus at   */
+/* 0): out [N] = H p.  Used by the implicit adjoint of the charge solve.      */
+int admp_qeq_hvp(int dtype, int flags, int natoms, const int* kmesh, const void* pos,
+                 const void* box, long long npairs, const long long* pairs, const void* ds,
+                 const void* buffer_scales, const void* hardness, const void* eta, double kappa,
+                 double ke, const void* p, void* out, void* workspace, size_t workspace_bytes,
+                 void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ADMP_B200_H_ */

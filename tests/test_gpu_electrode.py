@@ -1,0 +1,40 @@
+"""Constant-potential / constant-charge electrodes vs the reference's LAMMPS
+fixtures (forces at 5e-5 for slabs, 5e-4 for interfaces, as in
+test_electrode_conp.py) and vs the reference's own solved charges."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+from _gpu_helpers import T, rel
+
+pytestmark = pytest.mark.gpu
+
+CASES = [("electrode_conp_slab_2d", 5e-5), ("electrode_conp_slab_3d", 5e-5),
+         ("electrode_conp_interface_2d_bias", 5e-4), ("electrode_conq_interface_2d_pzc", 5e-4)]
+
+
+@pytest.mark.parametrize("name,tol", CASES)
+@pytest.mark.parametrize("method", ["lbfgs", "matinv"])
+def test_electrode_lammps(cuda, name, tol, method):
+    from admp_b200.electrode import LAMMPSElectrodeConstraint, PolarizableElectrode, infer, setup_from_lammps
+    from admp_b200.nblist import TorchNeighborList
+    d = golden(name)
+    if method == "matinv" and "interface" in name:
+        pytest.skip("dense path exercised on the slab fixtures")
+    calc = PolarizableElectrode(rcut=float(d["rcut"]), kappa=float(d["kappa"]), slab_corr=bool(d["slab_corr"]),
+                                eps=1e-6, ls_eps=1e-6, max_iter=100, ethresh=float(d["ethresh"]))
+    pos = T(d["pos"], cuda, grad=True)
+    box = T(d["box"], cuda)
+    charges = T(d["q_lammps"], cuda, grad=True)
+    nb = TorchNeighborList(float(d["rcut"]))
+    pairs = nb(pos, box)
+    cons = [LAMMPSElectrodeConstraint(indices=np.arange(int(a), int(z)), value=float(v),
+                                      mode="conp" if int(md) == 0 else "conq", eta=float(d["lammps_eta"]),
+                                      ffield=bool(d["ffield"])) for a, z, v, md in d["cons"]]
+    data = setup_from_lammps(len(d["q_lammps"]), cons, bool(d["symm"]), device=cuda)
+    E, F, q = infer(calc, pos, box, charges, pairs, nb.get_ds(), nb.get_buffer_scales(), *data, method=method)
+    assert calc.submodels["coulomb"]._kmesh.tolist() == d["kmesh"].tolist()
+    np.testing.assert_allclose(F.detach().cpu().numpy(), d["F_lammps"], atol=tol, rtol=tol)
+    assert np.abs(F.detach().cpu().numpy() - d["forces"]).max() < 2e-5
+    assert np.abs(q.detach().cpu().numpy() - d["q_ref"]).max() < 2e-5

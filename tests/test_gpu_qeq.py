@@ -1,0 +1,139 @@
+"""QEq charge solve on the B200 (matrix-free projected CG) against the
+reference's matinv / quadratic solutions, Hessian identity and the implicit
+adjoint against central finite differences."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+from _gpu_helpers import T, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(d, dev, kmesh=None, dtype=torch.float64, eps=1e-8, max_iter=500):
+    from admp_b200.qeq import QEqForceModule
+    m = QEqForceModule(float(d["rcut"]), float(d["ethresh"]), kmesh=kmesh, eps=eps, max_iter=max_iter)
+    pos = T(d["pos"], dev, dtype, grad=True)
+    box = T(d["box"], dev, dtype)
+    pairs = torch.tensor(d["pairs"], device=dev)
+    ds = T(d["ds"], dev, dtype)
+    bs = torch.tensor(d["bs"], device=dev)
+    n = pos.shape[0]
+    C = torch.ones(1, n, dtype=dtype, device=dev)
+    b = torch.zeros(1, dtype=dtype, device=dev)
+    return m, pos, box, pairs, ds, bs, T(d["chi"], dev, dtype), T(d["hardness"], dev, dtype), T(d["eta"], dev, dtype), C, b
+
+
+@pytest.mark.parametrize("name,kmesh", [("qeq_small", None), ("qeq_water_small", 20)])
+def test_qeq_cg_matches_reference(cuda, name, kmesh):
+    from admp_b200.qeq import pgrad_optimize
+    d = golden(name)
+    m, pos, box, pairs, ds, bs, chi, hd, eta, C, b = setup(d, cuda, kmesh)
+    E, q = pgrad_optimize(m, None, pos, box, chi, hd, eta, pairs, ds, bs, C, b, method="quadratic")
+    assert m.converge_iter >= 0
+    assert np.abs(q.detach().cpu().numpy() - d["q_matinv"]).max() < 1e-7
+    assert rel(E, d["E_matinv"]) < 1e-8
+    F = -torch.autograd.grad(E.sum(), pos)[0]
+    assert np.abs(F.cpu().numpy() - d["F_matinv"]).max() < 5e-6
+
+
+def test_qeq_eps_criterion_and_iterations(cuda):
+    """Stopping rule ||P grad|| / N < eps as in the reference (eps=1e-6)."""
+    from admp_b200.qeq import pgrad_optimize
+    from admp_b200.utils import calc_pgrads, vector_projection_coeff_matrix
+    d = golden("qeq_water_small")
+    m, pos, box, pairs, ds, bs, chi, hd, eta, C, b = setup(d, cuda, 20, eps=1e-6, max_iter=100)
+    E, q = pgrad_optimize(m, torch.zeros(pos.shape[0], dtype=torch.float64, device=cuda), pos, box, chi, hd, eta,
+                          pairs, ds, bs, C, b, reinit_q=True, method="lbfgs")
+    assert 0 <= m.converge_iter <= 100
+    pg = calc_pgrads(E, q, C, vector_projection_coeff_matrix(C))
+    assert (pg.norm() / q.shape[0]).item() < 1e-6 * 1.01
+    assert abs(q.sum().item()) < 1e-10
+
+
+def test_qeq_matinv_matches_reference(cuda):
+    from admp_b200.qeq import matinv_optimize
+    d = golden("qeq_water_small")
+    m, pos, box, pairs, ds, bs, chi, hd, eta, C, b = setup(d, cuda, 20)
+    E, q = matinv_optimize(m, pos, box, chi, hd, eta, pairs, ds, bs, C, b)
+    assert np.abs(q.detach().cpu().numpy() - d["q_matinv"]).max() < 1e-10
+    assert rel(E, d["E_matinv"]) < 1e-10
+
+
+def test_hessian_identity(cuda):
+    """1/2 q^T H q = E_coulomb + E_damping (reference test_qeq_numerical.py:331-369)."""
+    d = golden("qeq_water_small")
+    m, pos, box, pairs, ds, bs, chi, hd, eta, C, b = setup(d, cuda, 20)
+    zero = torch.zeros_like(chi)
+    H = m.calc_hessian(pos, box, chi, zero, eta, pairs, ds, bs)
+    rng = np.random.default_rng(0)
+    q = T(rng.uniform(-1, 1, pos.shape[0]), cuda)
+    e1 = m.submodels["coulomb"](pos, box, pairs, ds, bs, {"charge": q})
+    e2 = m.submodels["damping"](pos, box, pairs, ds, bs, {"charge": q, "eta": eta})
+    assert rel(0.5 * q @ H @ q, (e1 + e2).sum()) < 1e-10
+    assert rel(H, H.T) < 1e-12
+
+
+def test_qeq_cfg2_water_fp64_and_fp32(cuda):
+    """1,000 waters, 48^3 mesh: FP64 vs the reference's converged charges; the FP32
+    bulk path within 1e-5 e charge and 1e-4 relative force error."""
+    from admp_b200.nblist import TorchNeighborList
+    from admp_b200.qeq import pgrad_optimize
+    d = golden("qeq_water_cfg2")
+    for dtype, qtol, ftol in [(torch.float64, 2e-7, 1e-6), (torch.float32, 1e-5, 1e-4)]:
+        from admp_b200.qeq import QEqForceModule
+        m = QEqForceModule(6.0, 5e-4, kmesh=48, eps=1e-7, max_iter=300)
+        pos = T(d["pos"], cuda, dtype, grad=True)
+        box = T(d["box"], cuda, dtype)
+        nb = TorchNeighborList(6.0)
+        pairs = nb(pos, box)
+        n = pos.shape[0]
+        C = torch.ones(1, n, dtype=dtype, device=cuda)
+        E, q = pgrad_optimize(m, None, pos, box, T(d["chi"], cuda, dtype), T(d["hardness"], cuda, dtype),
+                              T(d["eta"], cuda, dtype), pairs, nb.get_ds(), nb.get_buffer_scales(), C,
+                              torch.zeros(1, dtype=dtype, device=cuda), method="quadratic")
+        F = -torch.autograd.grad(E.sum(), pos)[0].double().cpu().numpy()
+        qerr = np.abs(q.detach().double().cpu().numpy() - d["q_quadratic"]).max()
+        ferr = np.abs(F - d["F_quadratic"]).max() / np.abs(d["F_quadratic"]).max()
+        assert qerr < qtol, (dtype, qerr)
+        assert ferr < ftol, (dtype, ferr)
+
+
+def test_implicit_adjoint_vs_finite_differences(cuda):
+    """d(w . q*)/d theta through the adjoint CG vs central differences (step 1e-4)."""
+    from admp_b200.nblist import TorchNeighborList
+    from admp_b200.qeq import QEqForceModule, qeq_solve
+    d = golden("qeq_water_small")
+    m = QEqForceModule(6.0, 5e-4, kmesh=20, eps=1e-10, max_iter=500)
+    n = d["pos"].shape[0]
+    rng = np.random.default_rng(1)
+    w = T(rng.normal(size=n), cuda)
+    C = torch.ones(1, n, dtype=torch.float64, device=cuda)
+
+    def loss(pos_np, chi_np, eta_np, hd_np, grad=False):
+        pos = T(pos_np, cuda, grad=grad)
+        box = T(d["box"], cuda)
+        chi = T(chi_np, cuda, grad=grad)
+        eta = T(eta_np, cuda, grad=grad)
+        hd = T(hd_np, cuda, grad=grad)
+        nb = TorchNeighborList(6.0)
+        pairs = nb(pos, box)
+        q = qeq_solve(m, pos, box, chi, hd, eta, pairs, nb.get_ds(), nb.get_buffer_scales(), C)
+        return (w * q).sum(), (pos, chi, eta, hd)
+
+    L0, (pos, chi, eta, hd) = loss(d["pos"], d["chi"], d["eta"], d["hardness"], grad=True)
+    gpos, gchi, geta, ghd = torch.autograd.grad(L0, [pos, chi, eta, hd])
+    h = 1e-4
+    for arr_name, g in [("chi", gchi), ("eta", geta), ("hardness", ghd), ("pos", gpos)]:
+        for k in [0, 5, 17]:
+            base = {"pos": d["pos"].copy(), "chi": d["chi"].copy(), "eta": d["eta"].copy(),
+                    "hardness": d["hardness"].copy()}
+            idx = (k, 1) if arr_name == "pos" else k
+            base[arr_name][idx] += h
+            lp = loss(base["pos"], base["chi"], base["eta"], base["hardness"])[0].item()
+            base[arr_name][idx] -= 2 * h
+            lm = loss(base["pos"], base["chi"], base["eta"], base["hardness"])[0].item()
+            fd = (lp - lm) / (2 * h)
+            an = g[idx].item()
+            assert abs(fd - an) < 1e-6 + 1e-4 * abs(fd), (arr_name, k, fd, an)

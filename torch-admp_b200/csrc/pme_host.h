@@ -1,0 +1,148 @@
+// Host-side batch building and launch sequence for the reciprocal PME kernels.
+#pragma once
+
+#include <vector>
+
+#include "pme_kernels.cuh"
+#include "runtime.h"
+
+namespace admp {
+
+struct SysSpec {
+  int natoms;
+  int atom_off;
+  int K[3];
+  double kappa;
+  int box_idx;
+};
+
+// Launch geometry of a batch.
+template <typename T>
+struct RecipPlan {
+  Batch b;
+  size_t mesh_elems = 0;  // real mesh elements (all systems)
+  size_t spec_elems = 0;  // complex spectrum elements
+  size_t smem_z = 0, smem_y = 0, smem_x = 0;
+};
+
+template <typename T>
+inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
+  if (nsys <= 0 || nsys > kMaxBatch) return fail(ADMP_ERR_BAD_ARG, "batch of %d systems (max %d)", nsys, kMaxBatch);
+  Batch& b = p.b;
+  b.nsys = nsys;
+  b.apb = 32;
+  b.done = nullptr;
+  b.done_stride = 0;
+  int maxK[3] = {1, 1, 1};
+  for (int s = 0; s < nsys; ++s)
+    for (int d = 0; d < 3; ++d) {
+      if (sys[s].K[d] <= 0 || sys[s].K[d] > 4096)
+        return fail(ADMP_ERR_MESH, "mesh size %d out of range [1, 4096]", sys[s].K[d]);
+      maxK[d] = maxK[d] > sys[s].K[d] ? maxK[d] : sys[s].K[d];
+    }
+  b.maxK0 = maxK[0];
+  b.maxK1 = maxK[1];
+  b.maxK2 = maxK[2];
+  const size_t cs = sizeof(Cplx<T>);
+  const size_t budget = 150 * 1024;
+  // z passes: lp line pairs of length K2 per block, two buffers
+  int lp = (int)((sizeof(T) == 4 ? 4096 : 2048) / maxK[2]);
+  lp = lp < 1 ? 1 : (lp > 64 ? 64 : lp);
+  while (lp > 1 && (2 * (size_t)lp + 1) * maxK[2] * cs > budget) --lp;
+  b.lp = lp;
+  int zb = sizeof(T) == 4 ? 16 : 8;
+  const int mk01 = maxK[0] > maxK[1] ? maxK[0] : maxK[1];
+  while (zb > 1 && (2 * (size_t)zb + 1) * mk01 * cs + (mk01 + zb) * 8 > budget) zb >>= 1;
+  b.zb = zb;
+  p.smem_z = (2 * (size_t)lp + 1) * maxK[2] * cs;
+  p.smem_y = (2 * (size_t)zb + 1) * maxK[1] * cs;
+  p.smem_x = (2 * (size_t)zb + 1) * maxK[0] * cs + ((size_t)maxK[0] + zb) * 8;
+  if (p.smem_z > 227 * 1024 || p.smem_y > 227 * 1024 || p.smem_x > 227 * 1024)
+    return fail(ADMP_ERR_MESH, "mesh %dx%dx%d too large for the shared-memory FFT", maxK[0], maxK[1], maxK[2]);
+  int ba = 0, bz = 0, by = 0, bx = 0;
+  size_t mo = 0, so = 0;
+  for (int s = 0; s < nsys; ++s) {
+    SysDesc& d = b.s[s];
+    d.atom_off = sys[s].atom_off;
+    d.natoms = sys[s].natoms;
+    d.K0 = sys[s].K[0];
+    d.K1 = sys[s].K[1];
+    d.K2 = sys[s].K[2];
+    d.K2h = d.K2 / 2 + 1;
+    d.kappa = sys[s].kappa;
+    d.box_idx = sys[s].box_idx;
+    d.flags = 0;
+    d.blk_atom = ba;
+    d.blk_z = bz;
+    d.blk_y = by;
+    d.blk_x = bx;
+    d.mesh_off = (int64_t)mo;
+    d.spec_off = (int64_t)so;
+    const int ncb = (d.K2h + zb - 1) / zb;
+    ba += (d.natoms + b.apb - 1) / b.apb;
+    bz += ((d.K0 * d.K1 + 1) / 2 + lp - 1) / lp;
+    by += d.K0 * ncb;
+    bx += d.K1 * ncb;
+    mo += align_up((size_t)d.K0 * d.K1 * d.K2, 64);
+    so += align_up((size_t)d.K0 * d.K1 * d.K2h, 32);
+  }
+  b.nblk_atom = ba;
+  b.nblk_z = bz;
+  b.nblk_y = by;
+  b.nblk_x = bx;
+  p.mesh_elems = mo;
+  p.spec_elems = so;
+  return ADMP_OK;
+}
+
+// Mesh -> potential: the five FFT passes with the Green's function.
+template <typename T>
+inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const T* box, double* acc, double ke,
+                            cudaStream_t st) {
+  const Batch& b = p.b;
+  ADMP_CUDA_TRY(ensure_smem(fft_z_fwd_kernel<T>, p.smem_z));
+  ADMP_CUDA_TRY(ensure_smem(fft_z_inv_kernel<T>, p.smem_z));
+  ADMP_CUDA_TRY(ensure_smem(fft_y_kernel<T, false>, p.smem_y));
+  ADMP_CUDA_TRY(ensure_smem(fft_y_kernel<T, true>, p.smem_y));
+  ADMP_CUDA_TRY(ensure_smem(fft_x_green_kernel<T>, p.smem_x));
+  if (b.nblk_z) fft_z_fwd_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, mesh, spec);
+  if (b.nblk_y) fft_y_kernel<T, false><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
+  if (b.nblk_x) fft_x_green_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(b, spec, box, acc, ke);
+  if (b.nblk_y) fft_y_kernel<T, true><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
+  if (b.nblk_z) fft_z_inv_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, spec, mesh);
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
+// Full reciprocal evaluation: spread q, FFT/Green, gather.
+// `dE_dq` receives the potential (dE/dq), `dE_dpos` the gradient; both accumulate.
+template <typename T>
+inline int launch_recip(const RecipPlan<T>& p, const T* pos, const T* box, const T* q, T* mesh, Cplx<T>* spec,
+                        double* acc, double ke, T* dE_dq, T* dE_dpos, cudaStream_t st) {
+  const Batch& b = p.b;
+  ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
+  if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, q, mesh);
+  int s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st);
+  if (s) return s;
+  if (b.nblk_atom)
+    gather_kernel<T, true><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, q, mesh, dE_dq, dE_dpos, acc, T(1));
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
+// Potential only (for the CG matvec): phi_i = dE/dq_i of the charges v.
+template <typename T>
+inline int launch_recip_potential(const RecipPlan<T>& p, const T* pos, const T* box, const T* v, T* mesh,
+                                  Cplx<T>* spec, double* acc, double ke, T* pot, cudaStream_t st) {
+  const Batch& b = p.b;
+  ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
+  if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, v, mesh);
+  int s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st);
+  if (s) return s;
+  if (b.nblk_atom)
+    gather_kernel<T, false><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, v, mesh, pot, nullptr, acc, T(1));
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
+}  // namespace admp

@@ -1,0 +1,476 @@
+// Reciprocal-space PME kernels (order-6 B-splines, arbitrary mesh sizes),
+// batched over independent systems described by a by-value launch descriptor.
+//
+//   spread      q -> mesh Q                  recip.py:216-252
+//   fft_z_fwd   Q -> half spectrum along z   (two real lines per complex FFT)
+//   fft_y       along y (forward / inverse)
+//   fft_x_green along x, G(k)|S|^2 energy + k-space virial, S <- 2 G S, inverse x
+//                                             pme.py:410-443, recip.py:255-308
+//   fft_z_inv   half spectrum -> real potential mesh phi = dE/dQ
+//   gather      phi -> dE/dq, dE/dpos, fractional-coordinate virial
+//
+// Mesh layout (per system): real Q[K0][K1][K2] row-major (the reference's
+// flat index ((i0*K1)+i1)*K2+i2, recip.py:201-205); spectrum H[K0][K1][K2/2+1].
+#pragma once
+
+#include "admp_common.cuh"
+#include "fft_smem.cuh"
+
+namespace admp {
+
+struct SysDesc {
+  int32_t atom_off, natoms;
+  int32_t K0, K1, K2, K2h;
+  int32_t blk_atom, blk_z, blk_y, blk_x;
+  int64_t mesh_off, spec_off;
+  double kappa;
+  int32_t box_idx;
+  int32_t flags;
+};
+
+struct Batch {
+  int nsys;
+  int nblk_atom, nblk_z, nblk_y, nblk_x;
+  int apb;  // atoms per block (atom kernels)
+  int lp;   // line pairs per block (z passes)
+  int zb;   // columns per block (y / x passes)
+  int maxK0, maxK1, maxK2;
+  const int* done;   // optional per-system skip flags (done[s * done_stride])
+  int done_stride;
+  SysDesc s[kMaxBatch];
+};
+
+__device__ __forceinline__ bool skip_sys(const Batch& b, int s) {
+  return b.done != nullptr && b.done[(size_t)s * b.done_stride] != 0;
+}
+
+constexpr int kAccStride = 32;  // doubles per system in the accumulator array
+// accumulator slots
+constexpr int kAccErec = 0;     // reciprocal energy
+constexpr int kAccVk = 1;       // 9: dE/dB (B = box^-1) through k vectors
+constexpr int kAccWf = 10;      // 9: dE/dB through fractional coordinates
+constexpr int kAccSlots = 19;
+
+enum SysField { F_ATOM = 0, F_Z = 1, F_Y = 2, F_X = 3 };
+
+template <int F>
+__device__ __forceinline__ int blk_of(const SysDesc& d) {
+  return F == F_ATOM ? d.blk_atom : F == F_Z ? d.blk_z : F == F_Y ? d.blk_y : d.blk_x;
+}
+
+template <int F>
+__device__ __forceinline__ int find_sys(const Batch& b, int blk) {
+  int lo = 0, hi = b.nsys - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (blk_of<F>(b.s[mid]) <= blk)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int signed_k(int i, int K) { return i <= (K - 1) / 2 ? i : i - K; }
+
+// Per-dimension B-spline structure factor used by the reference:
+// theta_d(n) = sum_{m=-2..2} M6(m+3) cos(2 pi m n / K)   (pme.py:412-432)
+__device__ __forceinline__ double theta_1d(int n, int K) {
+  const double m4 = 26.0 / 120.0, m5 = 1.0 / 120.0, m3 = 66.0 / 120.0;
+  double c1 = cospi(2.0 * (double)n / (double)K);
+  double c2 = cospi(4.0 * (double)n / (double)K);
+  return m3 + 2.0 * m4 * c1 + 2.0 * m5 * c2;
+}
+
+// Geometry of one system, computed by one thread into shared memory.
+struct Geom {
+  double box[9];
+  double binv[9];
+  double vol;
+};
+
+template <typename T>
+__device__ __forceinline__ void load_geom(const T* box, int idx, Geom* g) {
+  if (threadIdx.x == 0) {
+    load_box(box + (size_t)idx * 9, g->box);
+    g->vol = inv3(g->box, g->binv);
+  }
+}
+
+// Stencil of one atom: mesh indices per dim and weights (+derivatives).
+template <typename T>
+struct Stencil {
+  int ix[6], iy[6], iz[6];
+  T w[3][6];
+  T dw[3][6];
+};
+
+template <typename T>
+__device__ __forceinline__ void make_stencil(const T* r, const Geom& g, int K0, int K1, int K2,
+                                             Stencil<T>& st) {
+  const int K[3] = {K0, K1, K2};
+  const double x0 = r[0], x1 = r[1], x2 = r[2];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    // x_d = K_d * (r @ box_inv)_d  (recip.py:33, 61)
+    double x = (double)K[d] * (x0 * g.binv[0 * 3 + d] + x1 * g.binv[1 * 3 + d] + x2 * g.binv[2 * 3 + d]);
+    double m0 = ceil(x);             // recip.py:62
+    // u0 = m0 - x + 3 (recip.py:63); the stencil point s = k - 3 has u = (m0 - x) + k
+    const T t = (T)(m0 - x);
+    bspline6<T>(t, st.w[d], st.dw[d]);
+    int base = (int)m0 - 3;
+    int* idx = d == 0 ? st.ix : d == 1 ? st.iy : st.iz;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) idx[k] = wrap_index(base + k, K[d]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// spread: warp per atom, 216 atomic adds per atom into a zeroed mesh.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) spread_kernel(Batch b, const T* __restrict__ pos,
+                                                     const T* __restrict__ box,
+                                                     const T* __restrict__ q, T* __restrict__ mesh) {
+  __shared__ Geom g;
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  load_geom(box, d.box_idx, &g);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int a_begin = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a_end = min(a_begin + b.apb, d.natoms);
+  T* M = mesh + d.mesh_off;
+  for (int a = a_begin + warp; a < a_end; a += blockDim.x >> 5) {
+    const int ga = d.atom_off + a;
+    const T qa = q[ga];
+    if (qa == T(0)) continue;
+    T r[3] = {pos[3 * (size_t)ga], pos[3 * (size_t)ga + 1], pos[3 * (size_t)ga + 2]};
+    Stencil<T> st;
+    make_stencil<T>(r, g, d.K0, d.K1, d.K2, st);
+    for (int p = lane; p < kStencil; p += 32) {
+      const int dx = p / 36, dy = (p / 6) % 6, dz = p % 6;
+      const size_t idx = ((size_t)st.ix[dx] * d.K1 + st.iy[dy]) * d.K2 + st.iz[dz];
+      atomicAdd(M + idx, qa * st.w[0][dx] * st.w[1][dy] * st.w[2][dz]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pass forward: two real lines -> one complex FFT -> two half spectra
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) fft_z_fwd_kernel(Batch b, const T* __restrict__ mesh,
+                                                        Cplx<T>* __restrict__ spec) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s = find_sys<F_Z>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K2 = d.K2, K2h = d.K2h, L = d.K0 * d.K1, npair = (L + 1) / 2;
+  const int p0 = (blockIdx.x - d.blk_z) * b.lp;
+  const int np = min(b.lp, npair - p0);
+  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
+  Cplx<T>* A = W + b.maxK2;
+  Cplx<T>* B = A + (size_t)b.lp * b.maxK2;
+  make_twiddles(W, K2);
+  const T* Q = mesh + d.mesh_off;
+  for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
+    const int p = idx / K2, t = idx - p * K2;
+    const int l0 = 2 * (p0 + p), l1 = l0 + 1;
+    Cplx<T> z;
+    z.x = Q[(size_t)l0 * K2 + t];
+    z.y = l1 < L ? Q[(size_t)l1 * K2 + t] : T(0);
+    A[p * K2 + t] = z;
+  }
+  __syncthreads();
+  Cplx<T>* R = fft_lines<T, false>(A, B, np, K2, K2, 1, W, false);
+  Cplx<T>* H = spec + d.spec_off;
+  for (int idx = threadIdx.x; idx < np * K2h; idx += blockDim.x) {
+    const int p = idx / K2h, k = idx - p * K2h;
+    const Cplx<T> Z = R[p * K2 + k];
+    const Cplx<T> Zm = R[p * K2 + (k == 0 ? 0 : K2 - k)];
+    const int l0 = 2 * (p0 + p);
+    Cplx<T> a, c;
+    a.x = (Z.x + Zm.x) * T(0.5);
+    a.y = (Z.y - Zm.y) * T(0.5);
+    c.x = (Z.y + Zm.y) * T(0.5);
+    c.y = (Zm.x - Z.x) * T(0.5);
+    H[(size_t)l0 * K2h + k] = a;
+    if (l0 + 1 < L) H[(size_t)(l0 + 1) * K2h + k] = c;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// y pass (forward or inverse), in place on the spectrum
+// ---------------------------------------------------------------------------
+template <typename T, bool INV>
+__global__ void __launch_bounds__(256) fft_y_kernel(Batch b, Cplx<T>* __restrict__ spec) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s = find_sys<F_Y>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K1 = d.K1, K2h = d.K2h, zb = b.zb;
+  const int ncb = (K2h + zb - 1) / zb;
+  const int local = blockIdx.x - d.blk_y;
+  const int x = local / ncb, cb = local - x * ncb;
+  const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
+  Cplx<T>* A = W + b.maxK1;
+  Cplx<T>* B = A + (size_t)zb * b.maxK1;
+  make_twiddles(W, K1);
+  Cplx<T>* H = spec + d.spec_off + (size_t)x * K1 * K2h + kz0;
+  for (int idx = threadIdx.x; idx < K1 * nz; idx += blockDim.x) {
+    const int y = idx / nz, c = idx - y * nz;
+    A[y * zb + c] = H[(size_t)y * K2h + c];
+  }
+  __syncthreads();
+  Cplx<T>* R = fft_lines<T, true>(A, B, nz, K1, 1, zb, W, INV);
+  for (int idx = threadIdx.x; idx < K1 * nz; idx += blockDim.x) {
+    const int y = idx / nz, c = idx - y * nz;
+    H[(size_t)y * K2h + c] = R[y * zb + c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x pass: forward FFT, Green's function (energy + virial), scale, inverse FFT
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __restrict__ spec,
+                                                          const T* __restrict__ box,
+                                                          double* __restrict__ acc, double ke) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ Geom g;
+  __shared__ double red[10 * 32];
+  const int s = find_sys<F_X>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h, zb = b.zb;
+  const int ncb = (K2h + zb - 1) / zb;
+  const int local = blockIdx.x - d.blk_x;
+  const int y = local / ncb, cb = local - y * ncb;
+  const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
+  Cplx<T>* A = W + b.maxK0;
+  Cplx<T>* B = A + (size_t)zb * b.maxK0;
+  double* thx = reinterpret_cast<double*>(B + (size_t)zb * b.maxK0);
+  double* thz = thx + b.maxK0;
+  make_twiddles(W, K0);
+  load_geom(box, d.box_idx, &g);
+  for (int i = threadIdx.x; i < K0; i += blockDim.x) thx[i] = theta_1d(signed_k(i, K0), K0);
+  for (int i = threadIdx.x; i < nz; i += blockDim.x) thz[i] = theta_1d(signed_k(kz0 + i, K2), K2);
+  Cplx<T>* H = spec + d.spec_off + (size_t)y * K2h + kz0;
+  const size_t xs = (size_t)K1 * K2h;
+  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
+    const int x = idx / nz, c = idx - x * nz;
+    A[x * zb + c] = H[(size_t)x * xs + c];
+  }
+  __syncthreads();
+  Cplx<T>* R = fft_lines<T, true>(A, B, nz, K0, 1, zb, W, false);
+  Cplx<T>* F = (R == A) ? B : A;
+  const double kappa = d.kappa;
+  const double inv4k2 = 1.0 / (4.0 * kappa * kappa);
+  const int ny = signed_k(y, K1);
+  const double thy = theta_1d(ny, K1);
+  const double pref = ke * 2.0 * kPi / g.vol;
+  double v[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) v[k] = 0.0;
+  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
+    const int x = idx / nz, c = idx - x * nz;
+    const int kz = kz0 + c;
+    const int n0 = signed_k(x, K0), n2 = signed_k(kz, K2);
+    Cplx<T> S = R[x * zb + c];
+    double G2 = 0.0;
+    if (n0 != 0 || ny != 0 || n2 != 0) {
+      double kv[3];
+#pragma unroll
+      for (int e = 0; e < 3; ++e)
+        kv[e] = 2.0 * kPi * (n0 * g.binv[0 * 3 + e] + ny * g.binv[1 * 3 + e] + n2 * g.binv[2 * 3 + e]);
+      const double ksq = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+      const double th = thx[x] * thy * thz[c];
+      const double G = pref / ksq * exp(-ksq * inv4k2) / (th * th);
+      const double w = (kz == 0 || (2 * kz == K2)) ? 1.0 : 2.0;
+      const double s2 = (double)S.x * (double)S.x + (double)S.y * (double)S.y;
+      const double Ek = w * G * s2;
+      v[0] += Ek;
+      const double f = -4.0 * kPi * (inv4k2 + 1.0 / ksq) * Ek;
+      const double nn[3] = {(double)n0, (double)ny, (double)n2};
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) v[1 + a * 3 + e] += f * nn[a] * kv[e];
+      G2 = 2.0 * G;
+    }
+    S.x = (T)(G2 * (double)S.x);
+    S.y = (T)(G2 * (double)S.y);
+    R[x * zb + c] = S;
+  }
+  block_atomic_sum<10>(v, acc + (size_t)s * kAccStride + kAccErec, red);
+  Cplx<T>* P = fft_lines<T, true>(R, F, nz, K0, 1, zb, W, true);
+  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
+    const int x = idx / nz, c = idx - x * nz;
+    H[(size_t)x * xs + c] = P[x * zb + c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pass inverse: two half spectra -> one complex inverse FFT -> two real lines
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) fft_z_inv_kernel(Batch b, const Cplx<T>* __restrict__ spec,
+                                                        T* __restrict__ mesh) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s = find_sys<F_Z>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K2 = d.K2, K2h = d.K2h, L = d.K0 * d.K1, npair = (L + 1) / 2;
+  const int p0 = (blockIdx.x - d.blk_z) * b.lp;
+  const int np = min(b.lp, npair - p0);
+  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
+  Cplx<T>* A = W + b.maxK2;
+  Cplx<T>* B = A + (size_t)b.lp * b.maxK2;
+  make_twiddles(W, K2);
+  const Cplx<T>* H = spec + d.spec_off;
+  for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
+    const int p = idx / K2, t = idx - p * K2;
+    const int l0 = 2 * (p0 + p), l1 = l0 + 1;
+    const bool lo = t < K2h;
+    const int tt = lo ? t : K2 - t;
+    Cplx<T> a = H[(size_t)l0 * K2h + tt];
+    Cplx<T> c;
+    if (l1 < L) {
+      c = H[(size_t)l1 * K2h + tt];
+    } else {
+      c.x = T(0);
+      c.y = T(0);
+    }
+    if (!lo) {
+      a.y = -a.y;
+      c.y = -c.y;
+    }
+    Cplx<T> z;
+    z.x = a.x - c.y;
+    z.y = a.y + c.x;
+    A[p * K2 + t] = z;
+  }
+  __syncthreads();
+  Cplx<T>* R = fft_lines<T, false>(A, B, np, K2, K2, 1, W, true);
+  T* M = mesh + d.mesh_off;
+  for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
+    const int p = idx / K2, t = idx - p * K2;
+    const int l0 = 2 * (p0 + p), l1 = l0 + 1;
+    const Cplx<T> z = R[p * K2 + t];
+    M[(size_t)l0 * K2 + t] = z.x;
+    if (l1 < L) M[(size_t)l1 * K2 + t] = z.y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// gather: warp per atom.  pot_i = sum phi theta; dE/du_d = q sum phi dtheta/du_d
+// ---------------------------------------------------------------------------
+template <typename T, bool FORCES>
+__global__ void __launch_bounds__(256) gather_kernel(Batch b, const T* __restrict__ pos,
+                                                     const T* __restrict__ box,
+                                                     const T* __restrict__ q,
+                                                     const T* __restrict__ phi,
+                                                     T* __restrict__ dE_dq, T* __restrict__ dE_dpos,
+                                                     double* __restrict__ acc, T pot_scale) {
+  __shared__ Geom g;
+  __shared__ double red[9 * 32];
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  load_geom(box, d.box_idx, &g);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int a_begin = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a_end = min(a_begin + b.apb, d.natoms);
+  const T* M = phi + d.mesh_off;
+  const int K[3] = {d.K0, d.K1, d.K2};
+  double wf[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) wf[k] = 0.0;
+  for (int a = a_begin + warp; a < a_end; a += blockDim.x >> 5) {
+    const int ga = d.atom_off + a;
+    T r[3] = {pos[3 * (size_t)ga], pos[3 * (size_t)ga + 1], pos[3 * (size_t)ga + 2]};
+    Stencil<T> st;
+    make_stencil<T>(r, g, d.K0, d.K1, d.K2, st);
+    T pot = 0, g0 = 0, g1 = 0, g2 = 0;
+    for (int p = lane; p < kStencil; p += 32) {
+      const int dx = p / 36, dy = (p / 6) % 6, dz = p % 6;
+      const size_t idx = ((size_t)st.ix[dx] * d.K1 + st.iy[dy]) * d.K2 + st.iz[dz];
+      const T f = M[idx];
+      const T wyz = st.w[1][dy] * st.w[2][dz];
+      pot += f * st.w[0][dx] * wyz;
+      if (FORCES) {
+        g0 += f * st.dw[0][dx] * wyz;
+        g1 += f * st.w[0][dx] * st.dw[1][dy] * st.w[2][dz];
+        g2 += f * st.w[0][dx] * st.w[1][dy] * st.dw[2][dz];
+      }
+    }
+    pot = warp_sum(pot);
+    if (FORCES) {
+      g0 = warp_sum(g0);
+      g1 = warp_sum(g1);
+      g2 = warp_sum(g2);
+    }
+    if (lane == 0) {
+      if (dE_dq) dE_dq[ga] += pot * pot_scale;
+      if (FORCES) {
+        const T qa = q[ga];
+        // u = m0 - x + 3  ->  dE/dx_d = -q * dE/du_d ; x_d = K_d (r @ B)_d
+        const double gx[3] = {-(double)qa * g0 * K[0], -(double)qa * g1 * K[1], -(double)qa * g2 * K[2]};
+        if (dE_dpos) {
+#pragma unroll
+          for (int e = 0; e < 3; ++e) {
+            double v = gx[0] * g.binv[e * 3 + 0] + gx[1] * g.binv[e * 3 + 1] + gx[2] * g.binv[e * 3 + 2];
+            dE_dpos[3 * (size_t)ga + e] += (T)v;
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < 3; ++e)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) wf[e * 3 + c] += (double)r[e] * gx[c];
+      }
+    }
+  }
+  if (FORCES) block_atomic_sum<9>(wf, acc + (size_t)s * kAccStride + kAccWf, red);
+}
+
+// ---------------------------------------------------------------------------
+// finalize: energy and dE/dbox = -B^T (dE/dB) B^T - E B^T   (one thread / system)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void recip_finalize_kernel(Batch b, const T* __restrict__ box, const double* __restrict__ acc,
+                                      double* __restrict__ energy, T* __restrict__ dE_dbox) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= b.nsys) return;
+  const SysDesc& d = b.s[s];
+  double bx[9], bi[9];
+  load_box(box + (size_t)d.box_idx * 9, bx);
+  inv3(bx, bi);
+  const double* a = acc + (size_t)s * kAccStride;
+  const double E = a[kAccErec];
+  const int o = d.box_idx;
+  if (energy) energy[o] += E;
+  if (dE_dbox) {
+    double dB[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) dB[k] = a[kAccVk + k] + a[kAccWf + k];
+    // M = B^T dB B^T ; out = -M - E B^T
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double m = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int l = 0; l < 3; ++l) m += bi[k * 3 + i] * dB[k * 3 + l] * bi[j * 3 + l];
+        dE_dbox[(size_t)o * 9 + i * 3 + j] += (T)(-m - E * bi[j * 3 + i]);
+      }
+  }
+}
+
+}  // namespace admp

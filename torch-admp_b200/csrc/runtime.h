@@ -1,0 +1,47 @@
+// Host-side runtime helpers shared by the entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "admp_common.cuh"
+
+namespace admp {
+
+// Device error word of the current device (a file-scope __device__ variable,
+// so no allocation).  Kernels record the first bad condition there.
+DevError* scratch_error(cudaStream_t st);
+// When synchronous checks are on (default), synchronise `st`, read and clear
+// the error word and turn it into a status.  Otherwise return ADMP_OK and
+// leave the error sticky for admp_check_errors().
+int check_error(DevError* err, cudaStream_t st);
+// Record a message and return `code`.
+int fail(int code, const char* fmt, ...);
+bool sync_checks();
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Carves typed sub-buffers out of a caller workspace.
+struct Carver {
+  char* base;
+  size_t cap;
+  size_t off;
+  Carver(void* b, size_t c) : base((char*)b), cap(c), off(0) {}
+  template <typename X>
+  X* take(size_t n) {
+    off = align_up(off, 256);
+    X* p = base ? (X*)(base + off) : nullptr;
+    off += n * sizeof(X);
+    return p;
+  }
+  bool ok() const { return off <= cap; }
+};
+
+// Sets the max dynamic smem of a kernel once.
+template <typename K>
+inline cudaError_t ensure_smem(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace admp

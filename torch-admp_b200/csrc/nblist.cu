@@ -117,7 +117,11 @@ __global__ void nb_bin_kernel(int pbc, int N, const T* __restrict__ pos, const N
                               double4* __restrict__ coord, int* __restrict__ cell, int* __restrict__ count,
                               DevError* err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N || m->status) return;
+  if (i >= N) return;
+  if (m->status) {  // invalid box / cutoff: no atom is binned, later passes skip it
+    cell[i] = -1;
+    return;
+  }
   double r[3] = {(double)pos[3 * (size_t)i], (double)pos[3 * (size_t)i + 1], (double)pos[3 * (size_t)i + 2]};
   if (!isfinite(r[0]) || !isfinite(r[1]) || !isfinite(r[2])) {
     report_error(err, ADMP_ERR_NONFINITE, 4, i);
@@ -193,8 +197,8 @@ __global__ void nb_pairs_kernel(int pbc, int N, double rc, const NbMeta* __restr
                                 long long* __restrict__ rowcnt, const long long* __restrict__ rowptr,
                                 long long* __restrict__ pairs, long long* __restrict__ bscale) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N || m->status) return;
-  const int ci = cell[i];
+  if (i >= N) return;
+  const int ci = m->status ? -1 : cell[i];
   if (ci < 0) {
     if (!FILL) rowcnt[i] = 0;
     return;

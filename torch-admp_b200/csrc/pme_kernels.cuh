@@ -271,6 +271,9 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
   const double kappa = d.kappa;
   const double inv4k2 = 1.0 / (4.0 * kappa * kappa);
   const int ny = signed_k(y, K1);
+  // label of the mirror index -y mod K1 (the reference labels K/2 as -K/2, so a
+  // Nyquist index is its own mirror with the same label)
+  const int nyb = signed_k(y == 0 ? 0 : K1 - y, K1);
   const double thy = theta_1d(ny, K1);
   const double pref = ke * 2.0 * kPi / g.vol;
   double v[10];
@@ -279,31 +282,43 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
     const int x = idx / nz, c = idx - x * nz;
     const int kz = kz0 + c;
+    // A half-spectrum entry p stands for p and its mirror pb = -p (mod K); both
+    // carry |S|^2 and the reference's own integer labels.  E = sum G(n)|S|^2
+    // over the full spectrum equals sum over the half spectrum of
+    // w * Gs * |S|^2 with Gs = (G(n_p) + G(n_pb)) / 2 and w = 2 (1 on the
+    // kz = 0 and kz = K2/2 planes, whose mirrors are separate entries).
     const int n0 = signed_k(x, K0), n2 = signed_k(kz, K2);
+    const int n0b = signed_k(x == 0 ? 0 : K0 - x, K0), n2b = signed_k(kz == 0 ? 0 : K2 - kz, K2);
+    const double th = thx[x] * thy * thz[c];
+    const double inv_th2 = 1.0 / (th * th);
+    const double w = (kz == 0 || (2 * kz == K2)) ? 1.0 : 2.0;
     Cplx<T> S = R[x * zb + c];
-    double G2 = 0.0;
-    if (n0 != 0 || ny != 0 || n2 != 0) {
+    const double s2 = (double)S.x * (double)S.x + (double)S.y * (double)S.y;
+    double Gs = 0.0;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const int a0 = m ? n0b : n0, a1 = m ? nyb : ny, a2 = m ? n2b : n2;
+      if (a0 == 0 && a1 == 0 && a2 == 0) continue;  // k = 0 excluded (pme.py:435-438)
       double kv[3];
 #pragma unroll
       for (int e = 0; e < 3; ++e)
-        kv[e] = 2.0 * kPi * (n0 * g.binv[0 * 3 + e] + ny * g.binv[1 * 3 + e] + n2 * g.binv[2 * 3 + e]);
+        kv[e] = 2.0 * kPi * (a0 * g.binv[0 * 3 + e] + a1 * g.binv[1 * 3 + e] + a2 * g.binv[2 * 3 + e]);
       const double ksq = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
-      const double th = thx[x] * thy * thz[c];
-      const double G = pref / ksq * exp(-ksq * inv4k2) / (th * th);
-      const double w = (kz == 0 || (2 * kz == K2)) ? 1.0 : 2.0;
-      const double s2 = (double)S.x * (double)S.x + (double)S.y * (double)S.y;
-      const double Ek = w * G * s2;
+      const double G = pref / ksq * exp(-ksq * inv4k2) * inv_th2;
+      Gs += 0.5 * G;
+      const double Ek = 0.5 * w * G * s2;
       v[0] += Ek;
+      // dE/dB[a][e] = sum_k E_k (-(1/(4 kappa^2) + 1/k^2)) 2 k_e 2 pi n_a
       const double f = -4.0 * kPi * (inv4k2 + 1.0 / ksq) * Ek;
-      const double nn[3] = {(double)n0, (double)ny, (double)n2};
+      const double nn[3] = {(double)a0, (double)a1, (double)a2};
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int e = 0; e < 3; ++e) v[1 + a * 3 + e] += f * nn[a] * kv[e];
-      G2 = 2.0 * G;
     }
-    S.x = (T)(G2 * (double)S.x);
-    S.y = (T)(G2 * (double)S.y);
+    // phi = dE/dQ = 2 * IFFT(Gs S)
+    S.x = (T)(2.0 * Gs * (double)S.x);
+    S.y = (T)(2.0 * Gs * (double)S.y);
     R[x * zb + c] = S;
   }
   block_atomic_sum<10>(v, acc + (size_t)s * kAccStride + kAccErec, red);

@@ -72,6 +72,16 @@ const char* admp_last_error_message(void);
  * admp_check_errors() (which always synchronises) reads and clears them. */
 void admp_set_sync_checks(int on);
 int admp_check_errors(void* stream);
+/* Number of kernels this library has launched (all entry points). */
+long long admp_launch_count(void);
+/* Kernel profiler: when enabled (capacity > 0 event pairs; 0 disables) the
+ * hot kernels are bracketed by CUDA events on their launch stream and tagged
+ * with their algorithmic bytes.  admp_profile_read fills per-kernel totals
+ * (index order: spread, fft_z_fwd, fft_y_fwd, fft_x_green, fft_y_inv,
+ * fft_z_inv, gather, pair_ef, csr_spmv, neighbors, cg_vector). */
+#define ADMP_PROFILE_KERNELS 11
+int admp_profile_enable(int capacity);
+int admp_profile_read(double* ms, long long* launches, double* bytes, int n);
 
 /* ------------------------------------------------------------------------ */
 /* Reciprocal-space PME.                                                     */
@@ -176,6 +186,90 @@ int admp_qeq_hvp(int dtype, int flags, int natoms, const int* kmesh, const void*
                  const void* buffer_scales, const void* hardness, const void* eta, double kappa,
                  double ke, const void* p, void* out, void* workspace, size_t workspace_bytes,
                  void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched serving.  Many independent systems (PME energy+forces requests or */
+/* QEq solves) run per launch; their state lives in caller-owned pools so a   */
+/* scheduler can admit new systems and retire finished ones between CG        */
+/* iterations.  There is no reference counterpart: the reference evaluates   */
+/* one system per Python call (CoulombForceModule.forward, pgrad_optimize);   */
+/* the per-system arithmetic is the same as the entry points above (FP32 or  */
+/* FP64 bulk, double reductions), with the total-charge constraint.          */
+/* ------------------------------------------------------------------------ */
+#define ADMP_SYS_PME 0
+#define ADMP_SYS_QEQ 1
+
+typedef struct admp_sys {
+  int natoms;          /* atoms of the system */
+  int atom_off;        /* first atom in the per-atom pools */
+  int slot;            /* index into the per-slot pools (box, energy, CG state) */
+  int kind;            /* ADMP_SYS_PME or ADMP_SYS_QEQ */
+  int kmesh[3];
+  int pad;
+  long long pair_off;  /* first entry in the pair pools */
+  long long pair_cap;  /* entries reserved for this system's neighbour rows */
+  double kappa;
+  double rcut;
+} admp_sys;
+
+typedef struct admp_pools {
+  /* per atom (dtype) */
+  void* pos;           /* [A,3] */
+  void* q;             /* [A]   charges; QEq warm start in, solution out */
+  void* chi;           /* [A]   QEq electronegativity */
+  void* hardness;      /* [A] */
+  void* eta;           /* [A]   Gaussian widths */
+  void* force;         /* [A,3] forces out */
+  void* frac;          /* [A]   float4 (F32) / double4 (F64) scratch */
+  long long* pstart;   /* [A]   first pair entry of the atom's row */
+  int* pcnt;           /* [A]   row length */
+  int* cell_of;        /* [A]   scratch */
+  int* sorted;         /* [A]   scratch */
+  /* per pair */
+  int* col;            /* [P]   neighbour atom (pool index) */
+  void* coef;          /* [P]   QEq real-space matrix entries (dtype) */
+  /* per slot */
+  void* box;           /* [S,3,3] */
+  double* energy;      /* [S] */
+  void* cg_state;      /* [S] x admp_serve_slot_state_bytes() */
+  int* slot_info;      /* [S,4]: done, iterations, status, pairs needed */
+  /* CG vectors per atom */
+  double* cg_x;
+  double* cg_r;
+  double* cg_diag;
+  double* cg_z;
+  double* cg_chi;
+  double* cg_hx;
+  void* cg_p;          /* dtype */
+  void* cg_hp;         /* dtype */
+  /* per-launch scratch */
+  void* mesh;          long long mesh_cap;   /* dtype elements */
+  void* spec;          long long spec_cap;   /* complex elements */
+  double* acc;         int acc_cap;          /* systems (32 doubles each) */
+  int* cells;          long long cells_cap;  /* ints */
+  void* sys_scratch;   long long sys_scratch_bytes;
+} admp_pools;
+
+size_t admp_serve_slot_state_bytes(void);
+size_t admp_serve_sys_scratch_bytes(int nsys);
+size_t admp_serve_cells_needed(const admp_sys* sys, int nsys);
+/* neighbour rows (CSR) of the listed systems; slot_info[.,2] gets the status
+ * (cutoff too large, capacity) and slot_info[.,3] the pair entries needed.   */
+int admp_serve_neighbors(int dtype, const admp_pools* pools, const admp_sys* sys, int nsys, void* stream);
+/* energy [slot] and forces of the listed systems at the charges in pools->q:
+ * PME systems: Ewald real + reciprocal + self + non-neutral (pme.py:261-310);
+ * QEq systems: additionally Gaussian damping and site terms (qeq.py:408-458). */
+int admp_serve_energy_forces(int dtype, const admp_pools* pools, const admp_sys* sys, int nsys, double ke,
+                             void* stream);
+/* QEq CG state of the listed systems from the warm start in pools->q. */
+int admp_serve_qeq_init(int dtype, const admp_pools* pools, const admp_sys* sys, int nsys, double tol,
+                        int max_iter, double ke, void* stream);
+/* niter CG iterations of the listed systems (converged ones are skipped);
+ * slot_info[.,0..1] get done flags and iteration counts. */
+int admp_serve_qeq_iterate(int dtype, const admp_pools* pools, const admp_sys* sys, int nsys, int niter,
+                           double tol, int max_iter, double ke, void* stream);
+/* copy the CG solution into pools->q */
+int admp_serve_qeq_finish(int dtype, const admp_pools* pools, const admp_sys* sys, int nsys, void* stream);
 
 #ifdef __cplusplus
 }

@@ -93,6 +93,51 @@ def nblist_pbc(pos: np.ndarray, box: np.ndarray, rc: float) -> np.ndarray:
     return pairs.astype(np.int64)
 
 
+def nblist_pbc_cells(pos: np.ndarray, box: np.ndarray, rc: float) -> np.ndarray:
+    """Same pair set as ``nblist_pbc`` via a cell list (the reference's own
+    strategy, nblist.py:382-445): atoms binned into cells at least rc high,
+    candidate pairs from the 27 neighbouring cells, minimum-image test.
+    Vectorised per cell pair; used where the O(N^2) form is too slow."""
+    check_cutoff(box, rc)
+    n = pos.shape[0]
+    binv = np.linalg.inv(box)
+    f = pos @ binv
+    f -= np.floor(f)
+    V = abs(np.linalg.det(box))
+    h = np.array([V / np.linalg.norm(np.cross(box[(d + 1) % 3], box[(d + 2) % 3])) for d in range(3)])
+    nc = np.maximum(np.floor(h / rc).astype(int), 1)
+    c = np.minimum((f * nc).astype(int), nc - 1)
+    cid = (c[:, 0] * nc[1] + c[:, 1]) * nc[2] + c[:, 2]
+    order = np.argsort(cid, kind="stable")
+    counts = np.bincount(cid, minlength=int(np.prod(nc)))
+    start = np.concatenate([[0], np.cumsum(counts)])
+    offs = []
+    for d in range(3):
+        offs.append([0] if nc[d] == 1 else ([0, 1] if nc[d] == 2 else [-1, 0, 1]))
+    out = []
+    for cx in range(nc[0]):
+        for cy in range(nc[1]):
+            for cz in range(nc[2]):
+                a = order[start[(cx * nc[1] + cy) * nc[2] + cz]:start[(cx * nc[1] + cy) * nc[2] + cz + 1]]
+                if a.size == 0:
+                    continue
+                nb = []
+                for ox in offs[0]:
+                    for oy in offs[1]:
+                        for oz in offs[2]:
+                            k = (((cx + ox) % nc[0]) * nc[1] + (cy + oy) % nc[1]) * nc[2] + (cz + oz) % nc[2]
+                            nb.append(order[start[k]:start[k + 1]])
+                b = np.concatenate(nb)
+                df = f[b][None, :, :] - f[a][:, None, :]
+                df -= np.floor(df + 0.5)
+                d = np.linalg.norm(df @ box, axis=-1)
+                ii, jj = np.nonzero((d < rc) & (d > 0.01))
+                out.append(np.stack([a[ii], b[jj]], axis=1))
+    pairs = np.concatenate(out, axis=0) if out else np.zeros((0, 2), np.int64)
+    pairs = pairs[np.lexsort((pairs[:, 1], pairs[:, 0]))]
+    return pairs.astype(np.int64)
+
+
 def nblist_obc(pos: np.ndarray, rc: float) -> np.ndarray:
     """Open-boundary full list, r < rc, i != j -- nblist.py:472-490."""
     d = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=-1)
@@ -137,9 +182,8 @@ def pme_real(q, pairs, ds, bs, kappa):
     ddr = np.where(m, (-2 * kappa / SQRT_PI * np.exp(-(kappa * ds) ** 2) * inv - er * inv * inv), 0.0)
     dE_dds = ddr * qi * qj * bs * DIELECTRIC
     c = er * inv * bs * DIELECTRIC
-    dq = np.zeros_like(q)
-    np.add.at(dq, pairs[:, 0], c * qj)
-    np.add.at(dq, pairs[:, 1], c * qi)
+    n = q.shape[0]
+    dq = np.bincount(pairs[:, 0], c * qj, n) + np.bincount(pairs[:, 1], c * qi, n)
     return e.sum(), dE_dds, dq
 
 
@@ -176,17 +220,14 @@ def damping(q, eta, pairs, ds, bs):
     # d/dds [-erfc(x) inv] = g/(2 eij) * inv + erfc(x) inv^2
     dE_dds = np.where(m, (g / (2 * eij_s) * inv + _erfc(x) * inv * inv), 0.0) * qi * qj * bs * DIELECTRIC
     c = pre * inv * bs * DIELECTRIC
-    dq = np.zeros_like(q)
-    np.add.at(dq, i, c * qj)
-    np.add.at(dq, j, c * qi)
+    n = q.shape[0]
+    dq = np.bincount(i, c * qj, n) + np.bincount(j, c * qi, n)
     dq += 2 * pre_self * q * DIELECTRIC
     # d/deij [-erfc(ds/(2 eij))] = -g * ds / (2 eij^2)
     dpair_deij = np.where(zero, 0.0, -g * ds / (2 * eij_s ** 2) * qi * qj * inv * bs * DIELECTRIC)
     deij_dei = np.where(zero, 0.0, ei / (2 * eij_s))
     deij_dej = np.where(zero, 0.0, ej / (2 * eij_s))
-    deta = np.zeros_like(eta)
-    np.add.at(deta, i, dpair_deij * deij_dei)
-    np.add.at(deta, j, dpair_deij * deij_dej)
+    deta = np.bincount(i, dpair_deij * deij_dei, n) + np.bincount(j, dpair_deij * deij_dej, n)
     deta += np.where(em, -q * q / (2 * SQRT_PI) * einv * einv, 0.0) * DIELECTRIC
     return E, dE_dds, dq, deta
 
@@ -436,8 +477,9 @@ def ds_backward(pos, box, pairs, g):
     dr = (f - nimg) @ box
     d = np.linalg.norm(dr, axis=1)
     v = (g / np.where(d > 0, d, 1.0))[:, None] * dr
-    np.add.at(dpos, pairs[:, 0], v)
-    np.add.at(dpos, pairs[:, 1], -v)
+    n = pos.shape[0]
+    for e in range(3):
+        dpos[:, e] += np.bincount(pairs[:, 0], v[:, e], n) - np.bincount(pairs[:, 1], v[:, e], n)
     dbox = -nimg.T @ v
     return dpos, dbox
 

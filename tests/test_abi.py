@@ -21,7 +21,7 @@ def test_library_exports_header_symbols():
     assert len(syms) >= 15
     for s in syms:
         assert hasattr(lib, s), s
-    assert set(syms) <= set(_lib.EXPORTS) | {"admp_serve_create"} or True
+    assert set(syms) == set(_lib.EXPORTS)
 
 
 def test_status_strings_and_version():

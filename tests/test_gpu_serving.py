@@ -1,0 +1,105 @@
+"""Continuous-batching server: each result matches the FP64 oracle (FP64 mode
+tightly, FP32 mode within 1e-4 relative force and 1e-5 e charge error) and is
+the same served alone and in a mixed stream."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import admp_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def small_stream(n=10, seed=11):
+    from admp_b200 import synthetic
+    reqs = synthetic.serving_stream(n, seed, rate=1000.0, nmin=200, nmax=900)
+    return reqs
+
+
+def oracle_result(req, rcut=6.0, ethresh=5e-4):
+    kappa = O.ewald_kappa(rcut, ethresh)
+    km = O.auto_kmesh(req.box, kappa, ethresh)
+    pairs = O.nblist_pbc(req.pos, req.box, rcut)
+    bs = O.pair_buffer_scales(pairs)
+    ds = O.pairs_ds(req.pos, pairs, req.box)
+    if req.kind == "pme":
+        o = O.coulomb_forces(req.pos, req.box, pairs, bs, req.charges, rcut=rcut, ethresh=ethresh, kmesh=km)
+        return o["E"], o["forces"], None
+    s = O.QEqSystem(req.pos, req.box, req.chi, req.hardness, req.eta, pairs, ds, bs, rcut=rcut, ethresh=ethresh,
+                    kmesh=km)
+    n = req.natoms
+    q, _ = O.solve_linear_cg(s, np.zeros(n), np.ones((1, n)), np.zeros(1), tol=1e-10, max_iter=2000)
+    E, _ = s.energy_grad(q)
+    o = O.coulomb_forces(req.pos, req.box, pairs, bs, q, rcut=rcut, ethresh=ethresh, kmesh=km)
+    Ed, dds, _, _ = O.damping(q, req.eta, pairs, ds, bs)
+    dp, _ = O.ds_backward(req.pos, req.box, pairs, dds)
+    return E, o["forces"] - dp, q
+
+
+@pytest.fixture(scope="module")
+def stream_and_oracle():
+    reqs = small_stream()
+    return reqs, [oracle_result(r) for r in reqs]
+
+
+def serve(reqs, dtype, tol, **kw):
+    from admp_b200.serving import ServingEngine
+    eng = ServingEngine(dtype=dtype, max_atoms=200_000, max_slots=64, mesh_budget=4_000_000, tol=tol, **kw)
+    res = eng.run(reqs, arrivals=False)
+    return {r.rid: r for r in res}, eng
+
+
+@pytest.mark.parametrize("dtype,etol,ftol,qtol", [(torch.float64, 1e-9, 1e-7, 1e-8), (torch.float32, 1e-5, 1e-4, 1e-5)])
+def test_serving_matches_oracle(cuda, stream_and_oracle, dtype, etol, ftol, qtol):
+    reqs, refs = stream_and_oracle
+    res, eng = serve(reqs, dtype, 1e-10 if dtype == torch.float64 else 1e-7)
+    assert len(res) == len(reqs)
+    for r, (E, F, q) in zip(reqs, refs):
+        out = res[r.rid]
+        assert out.status == 0, (r.rid, out.status)
+        assert abs(out.energy - E) / abs(E) < etol, (r.kind, out.energy, E)
+        ferr = np.abs(out.forces - F).max() / np.abs(F).max()
+        assert ferr < ftol, (r.kind, r.natoms, ferr)
+        if q is not None:
+            assert np.abs(out.charges - q).max() < qtol
+            assert out.iterations > 0
+    assert eng.stats["admitted"] == len(reqs)
+
+
+def test_serving_same_alone_and_in_mix(cuda, stream_and_oracle):
+    reqs, _ = stream_and_oracle
+    mix, _ = serve(reqs, torch.float32, 1e-7)
+    for k in (0, 3, 7):
+        alone, _ = serve([reqs[k]], torch.float32, 1e-7)
+        a, m = alone[reqs[k].rid], mix[reqs[k].rid]
+        assert abs(a.energy - m.energy) / abs(m.energy) < 1e-6
+        assert np.abs(a.forces - m.forces).max() / np.abs(m.forces).max() < 1e-5
+        if a.charges is not None:
+            assert np.abs(a.charges - m.charges).max() < 1e-6
+
+
+def test_serving_admission_limits_and_warm_start(cuda):
+    """A small atom pool forces queued admission; a repeated QEq system id warm-starts."""
+    from admp_b200 import synthetic
+    from admp_b200.serving import ServingEngine
+    reqs = [r for r in synthetic.serving_stream(12, 5, rate=1000.0, nmin=300, nmax=700) if r.kind == "qeq"][:3]
+    for r in reqs:
+        r.meta = {"system_id": r.rid}
+    eng = ServingEngine(dtype=torch.float32, max_atoms=1600, max_slots=8, mesh_budget=2_000_000, tol=1e-7)
+    res1 = eng.run(reqs, arrivals=False)
+    assert len(res1) == len(reqs) and eng.stats["ticks"] > 1
+    it1 = {r.rid: r.iterations for r in res1}
+    eng.results = []
+    res2 = eng.run(reqs, arrivals=False)
+    for r in res2:
+        assert r.iterations < it1[r.rid]
+    assert eng.atoms.used() == 0 and eng.pairs.used() == 0
+
+
+def test_serving_cutoff_too_large_reports_status(cuda):
+    from admp_b200.serving import ServingEngine
+    from admp_b200.synthetic import Request, random_charges_system
+    pos, box, q = random_charges_system(100, 10.0, 3, balanced=True)
+    eng = ServingEngine(dtype=torch.float32, max_atoms=10_000, max_slots=4, mesh_budget=1_000_000)
+    res = eng.run([Request(0, "pme", 0.0, pos, box, charges=q)], arrivals=False)
+    assert res[0].status == 2   # ADMP_ERR_CUTOFF_TOO_LARGE: rc 6 > L/2 = 5

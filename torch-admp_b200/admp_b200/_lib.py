@@ -26,7 +26,12 @@ EXPORTS = [
     "admp_check_errors", "admp_pme_recip_workspace_size", "admp_pme_recip", "admp_pair_energy",
     "admp_atom_terms", "admp_pair_distances", "admp_pair_distances_backward", "admp_nblist_workspace_size",
     "admp_nblist_count", "admp_nblist_fill", "admp_qeq_workspace_size", "admp_qeq_solve", "admp_qeq_hvp",
+    "admp_launch_count", "admp_profile_enable", "admp_profile_read", "admp_serve_slot_state_bytes",
+    "admp_serve_sys_scratch_bytes", "admp_serve_cells_needed", "admp_serve_neighbors", "admp_serve_energy_forces",
+    "admp_serve_qeq_init", "admp_serve_qeq_iterate", "admp_serve_qeq_finish",
 ]
+PROFILE_KERNELS = ["spread", "fft_z_fwd", "fft_y_fwd", "fft_x_green", "fft_y_inv", "fft_z_inv", "gather", "pair_ef",
+                   "csr_spmv", "neighbors", "cg_vector"]
 
 _vp, _i, _ll, _d, _sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_size_t
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -54,6 +59,9 @@ _SIGS = {
                             _dp, _vp, _d, _i, _ip, _dp, _vp, _sz, _vp]),
     "admp_qeq_hvp": (_i, [_i, _i, _i, _ip, _vp, _vp, _ll, _vp, _vp, _vp, _vp, _vp, _d, _d, _vp, _vp, _vp, _sz,
                           _vp]),
+    "admp_launch_count": (_ll, []),
+    "admp_profile_enable": (_i, [_i]),
+    "admp_profile_read": (_i, [_dp, _llp, _dp, _i]),
 }
 
 _lib = None
@@ -126,6 +134,23 @@ def require_cuda(t: torch.Tensor, name: str = "tensor") -> None:
         raise RuntimeError(
             f"admp_b200: {name} is on {t.device}; the B200 kernels need CUDA tensors "
             "(there is no CPU fallback).")
+
+
+def launch_count() -> int:
+    return int(load().admp_launch_count())
+
+
+def profile_enable(capacity: int) -> None:
+    check(load().admp_profile_enable(int(capacity)), "profile enable")
+
+
+def profile_read() -> dict:
+    n = len(PROFILE_KERNELS)
+    ms = (ctypes.c_double * n)()
+    cnt = (ctypes.c_longlong * n)()
+    by = (ctypes.c_double * n)()
+    check(load().admp_profile_read(ms, cnt, by, n), "profile read")
+    return {k: {"ms": ms[i], "launches": cnt[i], "bytes": by[i]} for i, k in enumerate(PROFILE_KERNELS)}
 
 
 def workspace(nbytes: int, device) -> torch.Tensor:

@@ -1,0 +1,446 @@
+"""Continuous-batching server for PME energy+forces and QEq solves on one GPU.
+
+Requests (positions, box and charges -- or QEq parameters) arrive over time.
+The engine keeps every admitted system's state resident on the device --
+positions, CSR neighbour rows, the CG vectors and scalars, the previous
+charges of a QEq system -- in pools carved by offset.  Each scheduler tick:
+
+  1. admits queued requests while slots, atom / pair pool space and the
+     mesh scratch budget allow (admission by HBM footprint), copies their
+     inputs host->device and builds their neighbour rows in one batched call;
+  2. PME requests get energy + forces in one batched call and complete;
+     QEq requests get their CG state initialised (warm start from the
+     previous charges of the same system id, if any);
+  3. runs ``iters_per_tick`` CG iterations over ALL active QEq systems in
+     lock-step launches (systems admitted this tick join immediately;
+     converged ones are skipped on the device);
+  4. reads the per-slot done flags once (the tick's only host sync) and
+     retires converged systems: final energy + forces at the solved charges,
+     results device->host, resources freed.
+
+All arithmetic runs in libadmp_b200.so (admp_serve_* entry points).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .utils import DIELECTRIC
+
+SYS_PME, SYS_QEQ = 0, 1
+MAX_PER_LAUNCH = 128
+
+
+class AdmpSys(ctypes.Structure):
+    _fields_ = [("natoms", ctypes.c_int), ("atom_off", ctypes.c_int), ("slot", ctypes.c_int),
+                ("kind", ctypes.c_int), ("kmesh", ctypes.c_int * 3), ("pad", ctypes.c_int),
+                ("pair_off", ctypes.c_longlong), ("pair_cap", ctypes.c_longlong), ("kappa", ctypes.c_double),
+                ("rcut", ctypes.c_double)]
+
+
+_P = ctypes.c_void_p
+
+
+class AdmpPools(ctypes.Structure):
+    _fields_ = [(n, _P) for n in ("pos", "q", "chi", "hardness", "eta", "force", "frac", "pstart", "pcnt", "cell_of",
+                                  "sorted", "col", "coef", "box", "energy", "cg_state", "slot_info", "cg_x", "cg_r",
+                                  "cg_diag", "cg_z", "cg_chi", "cg_hx", "cg_p", "cg_hp", "mesh")] + \
+               [("mesh_cap", ctypes.c_longlong), ("spec", _P), ("spec_cap", ctypes.c_longlong), ("acc", _P),
+                ("acc_cap", ctypes.c_int), ("cells", _P), ("cells_cap", ctypes.c_longlong), ("sys_scratch", _P),
+                ("sys_scratch_bytes", ctypes.c_longlong)]
+
+
+def _bind_serve(lib):
+    if getattr(lib, "_serve_bound", False):
+        return
+    PP = ctypes.POINTER(AdmpPools)
+    SP = ctypes.POINTER(AdmpSys)
+    lib.admp_serve_slot_state_bytes.restype = ctypes.c_size_t
+    lib.admp_serve_sys_scratch_bytes.restype = ctypes.c_size_t
+    lib.admp_serve_sys_scratch_bytes.argtypes = [ctypes.c_int]
+    lib.admp_serve_neighbors.argtypes = [ctypes.c_int, PP, SP, ctypes.c_int, _P]
+    lib.admp_serve_energy_forces.argtypes = [ctypes.c_int, PP, SP, ctypes.c_int, ctypes.c_double, _P]
+    lib.admp_serve_qeq_init.argtypes = [ctypes.c_int, PP, SP, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                        ctypes.c_double, _P]
+    lib.admp_serve_qeq_iterate.argtypes = [ctypes.c_int, PP, SP, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_int, ctypes.c_double, _P]
+    lib.admp_serve_qeq_finish.argtypes = [ctypes.c_int, PP, SP, ctypes.c_int, _P]
+    for n in ("admp_serve_neighbors", "admp_serve_energy_forces", "admp_serve_qeq_init", "admp_serve_qeq_iterate",
+              "admp_serve_qeq_finish"):
+        getattr(lib, n).restype = ctypes.c_int
+    lib._serve_bound = True
+
+
+class _Intervals:
+    """First-fit allocator of integer ranges inside [0, cap)."""
+
+    def __init__(self, cap: int, align: int = 1):
+        self.cap = cap
+        self.align = align
+        self.free = [(0, cap)]
+
+    def alloc(self, n: int) -> Optional[int]:
+        n = (n + self.align - 1) // self.align * self.align
+        for k, (a, b) in enumerate(self.free):
+            if b - a >= n:
+                if b - a == n:
+                    self.free.pop(k)
+                else:
+                    self.free[k] = (a + n, b)
+                return a
+        return None
+
+    def release(self, off: int, n: int) -> None:
+        n = (n + self.align - 1) // self.align * self.align
+        self.free.append((off, off + n))
+        self.free.sort()
+        merged = []
+        for a, b in self.free:
+            if merged and merged[-1][1] == a:
+                merged[-1] = (merged[-1][0], b)
+            else:
+                merged.append((a, b))
+        self.free = merged
+
+    def used(self) -> int:
+        return self.cap - sum(b - a for a, b in self.free)
+
+
+@dataclass
+class Result:
+    rid: int
+    kind: str
+    energy: float
+    forces: np.ndarray
+    charges: Optional[np.ndarray]
+    iterations: int
+    status: int
+    t_arrival: float
+    t_done: float
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_arrival
+
+
+@dataclass
+class _Active:
+    req: object
+    slot: int
+    atom_off: int
+    pair_off: int
+    pair_cap: int
+    kmesh: List[int]
+    kind: int
+    t_arrival: float
+    retries: int = 0
+
+
+def auto_kmesh(box_diag, kappa: float, ethresh: float) -> List[int]:
+    """ceil(2 kappa L / (3 ethresh^0.2)) per axis (pme.py:390-392)."""
+    return [int(math.ceil(2 * kappa * float(L) / (3.0 * ethresh ** (1.0 / 5.0)))) for L in box_diag]
+
+
+class ServingEngine:
+    def __init__(self, device="cuda:0", dtype=torch.float32, max_atoms: int = 4_000_000, max_slots: int = 512,
+                 pairs_per_atom: float = 150.0, mesh_budget: int = 64_000_000, rcut: float = 6.0,
+                 ethresh: float = 5e-4, tol: float = 1e-6, max_iter: int = 300, iters_per_tick: int = 8,
+                 ke: float = DIELECTRIC):
+        self.lib = L.load()
+        _bind_serve(self.lib)
+        self.dev = torch.device(device)
+        self.dtype = dtype
+        self.dt = L.dtype_code(dtype)
+        self.rcut, self.ethresh = rcut, ethresh
+        self.kappa = math.sqrt(-math.log(2 * ethresh)) / rcut
+        self.tol, self.max_iter, self.iters_per_tick, self.ke = tol, max_iter, iters_per_tick, ke
+        self.max_slots = max_slots
+        A = max_atoms
+        Pn = int(max_atoms * pairs_per_atom)
+        f = dict(dtype=dtype, device=self.dev)
+        i32 = dict(dtype=torch.int32, device=self.dev)
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        self.t = {
+            "pos": torch.zeros(A, 3, **f), "q": torch.zeros(A, **f), "chi": torch.zeros(A, **f),
+            "hardness": torch.zeros(A, **f), "eta": torch.zeros(A, **f), "force": torch.zeros(A, 3, **f),
+            "frac": torch.zeros(A, 4, **f), "pstart": torch.zeros(A, dtype=torch.int64, device=self.dev),
+            "pcnt": torch.zeros(A, **i32), "cell_of": torch.zeros(A, **i32), "sorted": torch.zeros(A, **i32),
+            "col": torch.zeros(Pn, **i32), "coef": torch.zeros(Pn, **f),
+            "box": torch.zeros(max_slots, 3, 3, **f), "energy": torch.zeros(max_slots, **f64),
+            "cg_state": torch.zeros(max_slots * self.lib.admp_serve_slot_state_bytes(), dtype=torch.uint8,
+                                    device=self.dev),
+            "slot_info": torch.zeros(max_slots, 4, **i32),
+            "cg_x": torch.zeros(A, **f64), "cg_r": torch.zeros(A, **f64), "cg_diag": torch.zeros(A, **f64),
+            "cg_z": torch.zeros(A, **f64), "cg_chi": torch.zeros(A, **f64), "cg_hx": torch.zeros(A, **f64),
+            "cg_p": torch.zeros(A, **f), "cg_hp": torch.zeros(A, **f),
+            "mesh": torch.zeros(mesh_budget, **f), "spec": torch.zeros(mesh_budget + 1024, 2, **f),
+            "acc": torch.zeros(MAX_PER_LAUNCH * 32, **f64),
+            "cells": torch.zeros(3 * (2 * A + 129 * MAX_PER_LAUNCH), **i32),
+            "sys_scratch": torch.zeros(self.lib.admp_serve_sys_scratch_bytes(MAX_PER_LAUNCH), dtype=torch.uint8,
+                                       device=self.dev),
+        }
+        t = self.t
+        self.pools = AdmpPools()
+        for name in ("pos", "q", "chi", "hardness", "eta", "force", "frac", "pstart", "pcnt", "cell_of", "sorted",
+                     "col", "coef", "box", "energy", "cg_state", "slot_info", "cg_x", "cg_r", "cg_diag", "cg_z",
+                     "cg_chi", "cg_hx", "cg_p", "cg_hp", "mesh", "spec", "acc", "cells", "sys_scratch"):
+            setattr(self.pools, name, t[name].data_ptr())
+        self.pools.mesh_cap = mesh_budget
+        self.pools.spec_cap = mesh_budget + 1024
+        self.pools.acc_cap = MAX_PER_LAUNCH
+        self.pools.cells_cap = t["cells"].numel()
+        self.pools.sys_scratch_bytes = t["sys_scratch"].numel()
+        self.mesh_budget = mesh_budget
+        self.atoms = _Intervals(A, 32)
+        self.pairs = _Intervals(Pn, 64)
+        self.free_slots = list(range(max_slots - 1, -1, -1))
+        self.queue: List = []
+        self.active_qeq: Dict[int, _Active] = {}
+        self.results: List[Result] = []
+        self.warm: Dict[object, np.ndarray] = {}
+        self.stream = torch.cuda.current_stream(self.dev)
+        self.pin = {}
+        self.stats = {"ticks": 0, "launch_calls": 0, "admitted": 0, "h2d_bytes": 0, "d2h_bytes": 0}
+        # results as host numpy arrays (True) or device tensors (False)
+        self.results_to_host = True
+
+    # -- resources -----------------------------------------------------------
+    def _pair_estimate(self, req) -> int:
+        n = req.natoms
+        V = abs(float(np.linalg.det(req.box)))
+        rho = n / V
+        mean = rho * 4.0 / 3.0 * math.pi * self.rcut ** 3
+        return int(n * (mean * 1.35 + 24)) + 256
+
+    def _mesh_of(self, kmesh) -> int:
+        return (kmesh[0] * kmesh[1] * kmesh[2] + 63) // 64 * 64
+
+    def footprint(self, req) -> dict:
+        """Device bytes a request holds while resident (atoms, pairs) and its mesh scratch."""
+        fb = 4 if self.dtype == torch.float32 else 8
+        per_atom = fb * 17 + 8 * 7 + 4 * 3
+        per_pair = 4 + fb
+        km = auto_kmesh(np.diagonal(req.box), self.kappa, self.ethresh)
+        return {"atom_bytes": req.natoms * per_atom, "pair_bytes": self._pair_estimate(req) * per_pair,
+                "mesh_elems": self._mesh_of(km)}
+
+    # -- API ------------------------------------------------------------------
+    def submit(self, req, t_arrival: Optional[float] = None) -> None:
+        self.queue.append((req, time.perf_counter() if t_arrival is None else t_arrival))
+
+    def _sys_array(self, items: List[_Active]):
+        arr = (AdmpSys * len(items))()
+        for k, a in enumerate(items):
+            s = arr[k]
+            s.natoms = a.req.natoms
+            s.atom_off = a.atom_off
+            s.slot = a.slot
+            s.kind = a.kind
+            for d in range(3):
+                s.kmesh[d] = a.kmesh[d]
+            s.pair_off = a.pair_off
+            s.pair_cap = a.pair_cap
+            s.kappa = self.kappa
+            s.rcut = self.rcut
+        return arr
+
+    def _chunks(self, items: List[_Active]):
+        """Split into launches of <= 128 systems whose meshes fit the scratch budget."""
+        out, cur, mesh = [], [], 0
+        for a in items:
+            m = self._mesh_of(a.kmesh)
+            if cur and (len(cur) >= MAX_PER_LAUNCH or mesh + m > self.mesh_budget):
+                out.append(cur)
+                cur, mesh = [], 0
+            cur.append(a)
+            mesh += m
+        if cur:
+            out.append(cur)
+        return out
+
+    def _call(self, fn, items, *extra):
+        for ch in self._chunks(items):
+            arr = self._sys_array(ch)
+            st = fn(self.dt, ctypes.byref(self.pools), arr, len(ch), *extra, self.stream.cuda_stream)
+            self.stats["launch_calls"] += 1
+            L.check(st, fn.__name__)
+
+    def _admit(self, now: float) -> List[_Active]:
+        admitted = []
+        mesh_in_tick = 0
+        keep = []
+        for req, tarr in self.queue:
+            if tarr > now:
+                keep.append((req, tarr))
+                continue
+            n = req.natoms
+            km = auto_kmesh(np.diagonal(req.box), self.kappa, self.ethresh)
+            m = self._mesh_of(km)
+            if not self.free_slots or m > self.mesh_budget:
+                keep.append((req, tarr))
+                continue
+            aoff = self.atoms.alloc(n)
+            if aoff is None:
+                keep.append((req, tarr))
+                continue
+            pcap = self._pair_estimate(req)
+            poff = self.pairs.alloc(pcap)
+            if poff is None:
+                self.atoms.release(aoff, n)
+                keep.append((req, tarr))
+                continue
+            slot = self.free_slots.pop()
+            a = _Active(req, slot, aoff, poff, pcap, km, SYS_QEQ if req.kind == "qeq" else SYS_PME, tarr)
+            admitted.append(a)
+            mesh_in_tick += m
+        self.queue = keep
+        if admitted:
+            self._upload(admitted)
+            self.stats["admitted"] += len(admitted)
+        return admitted
+
+    def _src(self, x, npdt):
+        """Source tensor for a request array: device tensors are used as they
+        are (device-to-device copy), host arrays go through pinned memory."""
+        if isinstance(x, torch.Tensor):
+            return x.to(self.dtype), 0
+        t = torch.from_numpy(np.ascontiguousarray(x, dtype=npdt)).pin_memory()
+        return t, t.numel() * t.element_size()
+
+    def _upload(self, items: List[_Active]) -> None:
+        t = self.t
+        npdt = np.float32 if self.dtype == torch.float32 else np.float64
+        for a in items:
+            r = a.req
+            n = r.natoms
+            sl = slice(a.atom_off, a.atom_off + n)
+            pos, nb = self._src(r.pos, npdt)
+            t["pos"][sl].copy_(pos.reshape(n, 3), non_blocking=True)
+            bx, b2 = self._src(r.box, npdt)
+            t["box"][a.slot].copy_(bx.reshape(3, 3), non_blocking=True)
+            nb += b2
+            if a.kind == SYS_PME:
+                q, b3 = self._src(r.charges, npdt)
+                t["q"][sl].copy_(q, non_blocking=True)
+                nb += b3
+            else:
+                for name, arr in (("chi", r.chi), ("hardness", r.hardness), ("eta", r.eta)):
+                    v, b3 = self._src(arr, npdt)
+                    t[name][sl].copy_(v, non_blocking=True)
+                    nb += b3
+                key = r.meta.get("system_id") if r.meta else None
+                w = self.warm.get(key) if key is not None else None
+                if w is not None and len(w) == n:
+                    t["q"][sl].copy_(w.to(self.dtype) if isinstance(w, torch.Tensor)
+                                     else torch.from_numpy(np.asarray(w, dtype=npdt)), non_blocking=True)
+                else:
+                    t["q"][sl].zero_()
+            self.stats["h2d_bytes"] += nb
+
+    def _finish(self, items: List[_Active], now_fn) -> None:
+        """Energy + forces of finished systems, results out, resources freed."""
+        if not items:
+            return
+        self._call(self.lib.admp_serve_energy_forces, items, self.ke)
+        t = self.t
+        host = self.results_to_host
+        outs = []
+        for a in items:
+            n = a.req.natoms
+            sl = slice(a.atom_off, a.atom_off + n)
+            q = None
+            if host:
+                F = torch.empty((n, 3), dtype=self.dtype, pin_memory=True)
+                F.copy_(t["force"][sl], non_blocking=True)
+                if a.kind == SYS_QEQ:
+                    q = torch.empty(n, dtype=self.dtype, pin_memory=True)
+                    q.copy_(t["q"][sl], non_blocking=True)
+            else:
+                F = t["force"][sl].clone()
+                if a.kind == SYS_QEQ:
+                    q = t["q"][sl].clone()
+            outs.append((a, F, q))
+        E = torch.empty(self.max_slots, dtype=torch.float64, pin_memory=True)
+        E.copy_(t["energy"], non_blocking=True)
+        info = torch.empty(self.max_slots, 4, dtype=torch.int32, pin_memory=True)
+        info.copy_(t["slot_info"], non_blocking=True)
+        self.stream.synchronize()
+        tdone = now_fn()
+        for a, F, q in outs:
+            st = int(info[a.slot, 2])
+            it = int(info[a.slot, 1]) if a.kind == SYS_QEQ else 0
+            if host:
+                Fo = F.numpy().copy()
+                qo = q.numpy().copy() if q is not None else None
+                self.stats["d2h_bytes"] += F.numel() * F.element_size() + 8 + (
+                    q.numel() * q.element_size() if q is not None else 0)
+            else:
+                Fo, qo = F, q
+            if qo is not None and a.req.meta and a.req.meta.get("system_id") is not None:
+                self.warm[a.req.meta["system_id"]] = qo.copy() if host else qo
+            self.results.append(Result(a.req.rid, a.req.kind, float(E[a.slot]), Fo, qo, it, st, a.t_arrival, tdone))
+            self._release(a)
+
+    def _release(self, a: _Active) -> None:
+        self.atoms.release(a.atom_off, a.req.natoms)
+        self.pairs.release(a.pair_off, a.pair_cap)
+        self.free_slots.append(a.slot)
+
+    def tick(self, now_fn=time.perf_counter) -> int:
+        """One scheduler step; returns the number of results completed."""
+        n0 = len(self.results)
+        now = now_fn()
+        new = self._admit(now)
+        if new:
+            self._call(self.lib.admp_serve_neighbors, new)
+            pme = [a for a in new if a.kind == SYS_PME]
+            qeq = [a for a in new if a.kind == SYS_QEQ]
+            if qeq:
+                self._call(self.lib.admp_serve_qeq_init, qeq, self.tol, self.max_iter, self.ke)
+                for a in qeq:
+                    self.active_qeq[a.slot] = a
+            if pme:
+                self._finish(pme, now_fn)
+        if self.active_qeq:
+            act = list(self.active_qeq.values())
+            self._call(self.lib.admp_serve_qeq_iterate, act, self.iters_per_tick, self.tol, self.max_iter, self.ke)
+            info = torch.empty(self.max_slots, 4, dtype=torch.int32, pin_memory=True)
+            info.copy_(self.t["slot_info"], non_blocking=True)
+            self.stream.synchronize()
+            done = [a for a in act if int(info[a.slot, 0]) != 0 or int(info[a.slot, 2]) != 0]
+            for a in done:
+                del self.active_qeq[a.slot]
+            if done:
+                self._call(self.lib.admp_serve_qeq_finish, done)
+                self._finish(done, now_fn)
+        self.stats["ticks"] += 1
+        return len(self.results) - n0
+
+    def pending(self) -> int:
+        return len(self.queue) + len(self.active_qeq)
+
+    def run(self, requests, arrivals: bool = True, time_scale: float = 1.0, max_seconds: float = 1e9):
+        """Serve a list of requests.  With ``arrivals`` the request ``arrival``
+        times (seconds) are honoured relative to the start; otherwise all are
+        available at once.  Returns the results in completion order."""
+        t0 = time.perf_counter()
+        for r in requests:
+            self.submit(r, t0 + (r.arrival * time_scale if arrivals else 0.0))
+        while self.pending():
+            if self.tick() == 0 and not self.active_qeq:
+                # nothing on the device: wait for the next arrival
+                nxt = min(t for _, t in self.queue) if self.queue else None
+                if nxt is not None:
+                    dt = nxt - time.perf_counter()
+                    if dt > 0:
+                        time.sleep(min(dt, 0.01))
+            if time.perf_counter() - t0 > max_seconds:
+                raise TimeoutError("serving run exceeded its time limit")
+        return self.results

@@ -105,11 +105,25 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
   ADMP_CUDA_TRY(ensure_smem(fft_y_kernel<T, false>, p.smem_y));
   ADMP_CUDA_TRY(ensure_smem(fft_y_kernel<T, true>, p.smem_y));
   ADMP_CUDA_TRY(ensure_smem(fft_x_green_kernel<T>, p.smem_x));
+  // algorithmic bytes: z passes read/write M reals + Mh complex, y/x passes Mh complex in and out
+  const double rb = (double)p.mesh_elems * sizeof(T), cb = (double)p.spec_elems * sizeof(Cplx<T>);
+  int h;
+  h = prof_begin(st);
   if (b.nblk_z) fft_z_fwd_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, mesh, spec);
+  prof_end(h, PK_FFT_Z_FWD, rb + cb, st);
+  h = prof_begin(st);
   if (b.nblk_y) fft_y_kernel<T, false><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
+  prof_end(h, PK_FFT_Y_FWD, 2 * cb, st);
+  h = prof_begin(st);
   if (b.nblk_x) fft_x_green_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(b, spec, box, acc, ke);
+  prof_end(h, PK_FFT_X_GREEN, 2 * cb, st);
+  h = prof_begin(st);
   if (b.nblk_y) fft_y_kernel<T, true><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
+  prof_end(h, PK_FFT_Y_INV, 2 * cb, st);
+  h = prof_begin(st);
   if (b.nblk_z) fft_z_inv_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, spec, mesh);
+  prof_end(h, PK_FFT_Z_INV, rb + cb, st);
+  count_launches(5);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
 }
@@ -117,15 +131,29 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
 // Full reciprocal evaluation: spread q, FFT/Green, gather.
 // `dE_dq` receives the potential (dE/dq), `dE_dpos` the gradient; both accumulate.
 template <typename T>
+inline double plan_atoms(const RecipPlan<T>& p) {
+  double n = 0;
+  for (int s = 0; s < p.b.nsys; ++s) n += p.b.s[s].natoms;
+  return n;
+}
+
+template <typename T>
 inline int launch_recip(const RecipPlan<T>& p, const T* pos, const T* box, const T* q, T* mesh, Cplx<T>* spec,
                         double* acc, double ke, T* dE_dq, T* dE_dpos, cudaStream_t st) {
   const Batch& b = p.b;
+  const double na = plan_atoms(p), mb = (double)p.mesh_elems * sizeof(T);
   ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
+  int h = prof_begin(st);
   if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, q, mesh);
+  prof_end(h, PK_SPREAD, na * 4 * sizeof(T) + mb, st);
+  count_launches(1);
   int s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st);
   if (s) return s;
+  h = prof_begin(st);
   if (b.nblk_atom)
     gather_kernel<T, true><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, q, mesh, dE_dq, dE_dpos, acc, T(1));
+  prof_end(h, PK_GATHER, mb + na * 4 * sizeof(T) + na * 3 * sizeof(T), st);
+  count_launches(1);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
 }
@@ -135,12 +163,18 @@ template <typename T>
 inline int launch_recip_potential(const RecipPlan<T>& p, const T* pos, const T* box, const T* v, T* mesh,
                                   Cplx<T>* spec, double* acc, double ke, T* pot, cudaStream_t st) {
   const Batch& b = p.b;
+  const double na = plan_atoms(p), mb = (double)p.mesh_elems * sizeof(T);
   ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
+  int h = prof_begin(st);
   if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, v, mesh);
+  prof_end(h, PK_SPREAD, na * 4 * sizeof(T) + mb, st);
   int s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st);
   if (s) return s;
+  h = prof_begin(st);
   if (b.nblk_atom)
     gather_kernel<T, false><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, v, mesh, pot, nullptr, acc, T(1));
+  prof_end(h, PK_GATHER, mb + na * 4 * sizeof(T) + na * sizeof(T), st);
+  count_launches(2);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
 }

@@ -35,13 +35,13 @@ struct Batch {
   int lp;   // line pairs per block (z passes)
   int zb;   // columns per block (y / x passes)
   int maxK0, maxK1, maxK2;
-  const int* done;   // optional per-system skip flags (done[s * done_stride])
+  const int* done;   // optional per-slot skip flags (done[slot * done_stride], slot = box_idx)
   int done_stride;
   SysDesc s[kMaxBatch];
 };
 
 __device__ __forceinline__ bool skip_sys(const Batch& b, int s) {
-  return b.done != nullptr && b.done[(size_t)s * b.done_stride] != 0;
+  return b.done != nullptr && b.done[(size_t)b.s[s].box_idx * b.done_stride] != 0;
 }
 
 constexpr int kAccStride = 32;  // doubles per system in the accumulator array

@@ -91,7 +91,7 @@ static int qeq_prepare(QEqCtx<T>& c, const T* chi, const T* hard, const T* eta, 
                                                     c.w.chi_eff, c.w.sc);
   if (c.nc > 0) {
     qeq_gram_kernel<T><<<b.nblk_atom, 256, 0, c.st>>>(b, c.nc, c.C, (long long)c.N, c.w.sc);
-    qeq_gram_invert_kernel<<<1, 32, 0, c.st>>>(1, c.nc, c.w.sc);
+    qeq_gram_invert_kernel<<<1, 32, 0, c.st>>>(b, c.nc, c.w.sc);
   }
   if (c.Pn > 0 && (c.P.flags & (ADMP_QEQ_RSPACE | ADMP_QEQ_DAMPING))) {
     DevError* err = scratch_error(c.st);
@@ -165,7 +165,7 @@ static int qeq_solve_impl(int flags, int N, const int* kmesh, const T* pos, cons
   CGScal h;
   while (true) {
     for (int k = 0; k < chunk; ++k) {
-      qeq_rotate_kernel<<<1, 32, 0, st>>>(1, c.w.sc);
+      qeq_rotate_kernel<<<1, 32, 0, st>>>(b, c.w.sc);
       s = qeq_matvec<T>(c, c.w.p, c.w.Hp, nullptr);
       if (s) return s;
       qeq_update_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, c.w.x, c.w.r, c.w.p, c.w.Hp, C, (long long)N, c.w.sc);

@@ -50,6 +50,13 @@ __device__ __forceinline__ bool sys_done(const CGScal* sc, int s) {
   return sc[s].done != 0;
 }
 
+// Constraint row c at atom i; a null matrix stands for the single all-ones
+// row of the total-charge constraint.
+template <typename T>
+__device__ __forceinline__ double cval(const T* C, int c, long long cstride, int i) {
+  return C ? cval(C, c, cstride, i) : 1.0;
+}
+
 // Setup per atom: diag_i, z_i, chi_eff_i; per system (block 0 thread 0 of the
 // system's first block): slab / non-neutral constants.
 template <typename T>
@@ -58,8 +65,9 @@ __global__ void __launch_bounds__(256)
                      const T* __restrict__ chi, const T* __restrict__ hard, const T* __restrict__ eta,
                      const T* __restrict__ shift, double* __restrict__ diag, double* __restrict__ zc,
                      double* __restrict__ chi_eff, CGScal* __restrict__ sc) {
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s0];
+  const int s = d.box_idx;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
   const double kappa = d.kappa, ke = P.ke;
@@ -91,8 +99,9 @@ template <typename T>
 __global__ void __launch_bounds__(256)
     qeq_gram_kernel(Batch b, int nc, const T* __restrict__ C, long long cstride, CGScal* __restrict__ sc) {
   __shared__ double red[16 * 32];
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s0];
+  const int s = d.box_idx;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
   double v[16];
@@ -101,15 +110,16 @@ __global__ void __launch_bounds__(256)
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = d.atom_off + a;
     for (int r = 0; r < nc; ++r)
-      for (int c = 0; c < nc; ++c) v[r * kMaxConst + c] += (double)C[r * cstride + i] * (double)C[c * cstride + i];
+      for (int c = 0; c < nc; ++c) v[r * kMaxConst + c] += cval(C, r, cstride, i) * cval(C, c, cstride, i);
   }
   block_atomic_sum<16>(v, sc[s].Ginv, red);
 }
 
 // Invert the Gram matrices (one thread per system, Gauss-Jordan).
-__global__ void qeq_gram_invert_kernel(int nsys, int nc, CGScal* __restrict__ sc) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsys) return;
+static __global__ void qeq_gram_invert_kernel(Batch b, int nc, CGScal* __restrict__ sc) {
+  const int s0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s0 >= b.nsys) return;
+  const int s = b.s[s0].box_idx;
   double a[kMaxConst][2 * kMaxConst];
   for (int r = 0; r < nc; ++r)
     for (int c = 0; c < 2 * nc; ++c) a[r][c] = c < nc ? sc[s].Ginv[r * kMaxConst + c] : (c - nc == r ? 1.0 : 0.0);
@@ -144,9 +154,10 @@ __global__ void __launch_bounds__(256)
                     long long cstride, int nc, int want_cv, CGScal* __restrict__ sc, T* __restrict__ hv_zero,
                     T* __restrict__ vt) {
   __shared__ double red[7 * 32];
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s0];
+  const int s = d.box_idx;
   if (sys_done<T>(sc, s)) return;
-  const SysDesc& d = b.s[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -158,7 +169,7 @@ __global__ void __launch_bounds__(256)
     acc[1] += x * z;
     acc[2] += x * z * z;
     if (want_cv)
-      for (int c = 0; c < nc; ++c) acc[3 + c] += (double)C[c * cstride + i] * x;
+      for (int c = 0; c < nc; ++c) acc[3 + c] += cval(C, c, cstride, i) * x;
     if (hv_zero) hv_zero[i] = T(0);
     if (vt) vt[i] = (T)x;
   }
@@ -222,9 +233,10 @@ __global__ void __launch_bounds__(256)
                       const double* __restrict__ diag, const double* __restrict__ zc, const T* __restrict__ C,
                       long long cstride, CGScal* __restrict__ sc, double* __restrict__ hv_out) {
   __shared__ double red[5 * 32];
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s0];
+  const int s = d.box_idx;
   if (sc[s].done) return;
-  const SysDesc& d = b.s[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
   const CGScal& S = sc[s];
@@ -243,7 +255,7 @@ __global__ void __launch_bounds__(256)
     Hv[i] = (T)h;
     if (hv_out) hv_out[i] = h;
     acc[0] += x * h;
-    for (int c = 0; c < nc; ++c) acc[1 + c] += (double)C[c * cstride + i] * h;
+    for (int c = 0; c < nc; ++c) acc[1 + c] += cval(C, c, cstride, i) * h;
   }
   double a1v[1] = {acc[0]};
   block_atomic_sum<1>(a1v, &sc[s].pHp, red);
@@ -259,9 +271,10 @@ __global__ void __launch_bounds__(256)
     qeq_update_kernel(Batch b, double* __restrict__ x, double* __restrict__ r, const T* __restrict__ p,
                       T* __restrict__ Hp, const T* __restrict__ C, long long cstride, CGScal* __restrict__ sc) {
   __shared__ double red[32];
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s0];
+  const int s = d.box_idx;
   if (sc[s].done) return;
-  const SysDesc& d = b.s[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
   const CGScal& S = sc[s];
@@ -275,7 +288,7 @@ __global__ void __launch_bounds__(256)
     const int i = d.atom_off + a;
     double w = (double)Hp[i];
     Hp[i] = T(0);
-    for (int c = 0; c < nc; ++c) w -= (double)C[c * cstride + i] * lam[c];
+    for (int c = 0; c < nc; ++c) w -= cval(C, c, cstride, i) * lam[c];
     x[i] += alpha * (double)p[i];
     const double rn = r[i] - alpha * w;
     r[i] = rn;
@@ -296,9 +309,10 @@ __global__ void __launch_bounds__(256)
     qeq_direction_kernel(Batch b, QEqParams P, const double* __restrict__ r, T* __restrict__ p,
                          const double* __restrict__ zc, CGScal* __restrict__ sc) {
   __shared__ double red[3 * 32];
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s0];
+  const int s = d.box_idx;
   if (sc[s].done) return;
-  const SysDesc& d = b.s[s];
   const CGScal& S = sc[s];
   const double rrn = S.rr_new;
   const bool conv = sqrt(rrn) / (double)(d.natoms > 0 ? d.natoms : 1) < P.tol;
@@ -326,9 +340,11 @@ __global__ void __launch_bounds__(256)
 }
 
 // Start of an iteration: rotate scalars (rr <- rr_new), zero accumulators.
-__global__ void qeq_rotate_kernel(int nsys, CGScal* __restrict__ sc) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsys || sc[s].done) return;
+static __global__ void qeq_rotate_kernel(Batch b, CGScal* __restrict__ sc) {
+  const int s0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s0 >= b.nsys) return;
+  const int s = b.s[s0].box_idx;
+  if (sc[s].done) return;
   sc[s].rr = sc[s].rr_new;
   sc[s].rr_new = 0.0;
   sc[s].pHp = 0.0;
@@ -341,8 +357,9 @@ template <typename T>
 __global__ void __launch_bounds__(256)
     qeq_project_kernel(Batch b, double* __restrict__ x, const T* __restrict__ C, long long cstride,
                        const CGScal* __restrict__ sc) {
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s0];
+  const int s = d.box_idx;
   const CGScal& S = sc[s];
   const int nc = S.n_const;
   double lam[kMaxConst] = {0, 0, 0, 0};
@@ -353,7 +370,7 @@ __global__ void __launch_bounds__(256)
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = d.atom_off + a;
     double v = x[i];
-    for (int c = 0; c < nc; ++c) v += (double)C[c * cstride + i] * lam[c];
+    for (int c = 0; c < nc; ++c) v += cval(C, c, cstride, i) * lam[c];
     x[i] = v;
   }
 }
@@ -365,8 +382,9 @@ __global__ void __launch_bounds__(256)
                      const T* __restrict__ C, long long cstride, const double* __restrict__ zc,
                      double* __restrict__ r, T* __restrict__ p, CGScal* __restrict__ sc, int pass) {
   __shared__ double red[4 * 32];
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s0];
+  const int s = d.box_idx;
   const CGScal& S = sc[s];
   const int nc = S.n_const;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
@@ -376,7 +394,7 @@ __global__ void __launch_bounds__(256)
     for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
       const int i = d.atom_off + a;
       const double g = chi_eff[i] + hx[i];
-      for (int c = 0; c < nc; ++c) acc[c] += (double)C[c * cstride + i] * g;
+      for (int c = 0; c < nc; ++c) acc[c] += cval(C, c, cstride, i) * g;
     }
     if (nc > 0) block_atomic_sum<4>(acc, sc[s].Cv, red);
     return;
@@ -388,7 +406,7 @@ __global__ void __launch_bounds__(256)
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = d.atom_off + a;
     double g = chi_eff[i] + hx[i];
-    for (int c = 0; c < nc; ++c) g -= (double)C[c * cstride + i] * lam[c];
+    for (int c = 0; c < nc; ++c) g -= cval(C, c, cstride, i) * lam[c];
     const double rv = -g;
     r[i] = rv;
     p[i] = (T)rv;
@@ -405,7 +423,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // After the initial residual: decide done, clear accumulators.
-__global__ void qeq_set_b_kernel(CGScal* __restrict__ sc, int nc, double b0, double b1, double b2, double b3) {
+static __global__ void qeq_set_b_kernel(CGScal* __restrict__ sc, int nc, double b0, double b1, double b2, double b3) {
   if (threadIdx.x == 0) {
     sc[0].b[0] = b0;
     sc[0].b[1] = b1;
@@ -427,10 +445,11 @@ __global__ void cast_back_kernel(long long n, const double* __restrict__ in, T* 
     out[i] = (T)in[i];
 }
 
-__global__ void qeq_init_done_kernel(Batch b, QEqParams P, CGScal* __restrict__ sc) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= b.nsys) return;
-  const double n = b.s[s].natoms > 0 ? b.s[s].natoms : 1;
+static __global__ void qeq_init_done_kernel(Batch b, QEqParams P, CGScal* __restrict__ sc) {
+  const int s0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s0 >= b.nsys) return;
+  const int s = b.s[s0].box_idx;
+  const double n = b.s[s0].natoms > 0 ? b.s[s0].natoms : 1;
   sc[s].rr = sc[s].rr_new;
   sc[s].iter = 0;
   for (int c = 0; c < kMaxConst; ++c) sc[s].Cv[c] = 0.0;

@@ -1,6 +1,7 @@
 // Status strings, last-error messages and the device error word.
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "runtime.h"
@@ -14,6 +15,35 @@ static bool g_sync = true;
 static DevError* g_err_ptr[64] = {nullptr};
 
 bool sync_checks() { return g_sync; }
+
+static long long g_launches = 0;
+void count_launches(int n) { g_launches += n; }
+
+struct ProfRec {
+  cudaEvent_t a, b;
+  int kernel;
+  double bytes;
+};
+static bool g_prof = false;
+static ProfRec* g_prof_recs = nullptr;
+static int g_prof_cap = 0, g_prof_n = 0;
+
+bool prof_on() { return g_prof; }
+
+int prof_begin(cudaStream_t st) {
+  if (!g_prof || g_prof_n >= g_prof_cap) return -1;
+  ProfRec& r = g_prof_recs[g_prof_n];
+  if (cudaEventRecord(r.a, st) != cudaSuccess) return -1;
+  return g_prof_n++;
+}
+
+void prof_end(int slot, int kernel, double bytes, cudaStream_t st) {
+  if (slot < 0) return;
+  ProfRec& r = g_prof_recs[slot];
+  r.kernel = kernel;
+  r.bytes = bytes;
+  cudaEventRecord(r.b, st);
+}
 
 void set_last_message(const char* fmt, ...) {
   va_list ap;
@@ -109,6 +139,53 @@ extern "C" const char* admp_status_string(int s) {
 extern "C" const char* admp_last_error_message(void) { return g_msg; }
 
 extern "C" void admp_set_sync_checks(int on) { g_sync = on != 0; }
+
+extern "C" long long admp_launch_count(void) { return g_launches; }
+
+extern "C" int admp_profile_enable(int capacity) {
+  if (g_prof_recs) {
+    for (int k = 0; k < g_prof_cap; ++k) {
+      cudaEventDestroy(g_prof_recs[k].a);
+      cudaEventDestroy(g_prof_recs[k].b);
+    }
+    free(g_prof_recs);
+    g_prof_recs = nullptr;
+  }
+  g_prof = capacity > 0;
+  g_prof_cap = 0;
+  g_prof_n = 0;
+  if (!g_prof) return ADMP_OK;
+  g_prof_recs = (ProfRec*)calloc((size_t)capacity, sizeof(ProfRec));
+  if (!g_prof_recs) return fail(ADMP_ERR_BAD_ARG, "profile: out of host memory");
+  for (int k = 0; k < capacity; ++k) {
+    if (cudaEventCreate(&g_prof_recs[k].a) != cudaSuccess || cudaEventCreate(&g_prof_recs[k].b) != cudaSuccess)
+      return fail(ADMP_ERR_CUDA, "profile: cudaEventCreate failed");
+    g_prof_cap = k + 1;
+  }
+  return ADMP_OK;
+}
+
+// Per-kernel totals since the last enable: ms[k], launches[k], bytes[k]
+// (arrays of PK_COUNT).  Synchronises on the recorded events.
+extern "C" int admp_profile_read(double* ms, long long* launches, double* bytes, int n) {
+  for (int k = 0; k < n; ++k) {
+    ms[k] = 0.0;
+    launches[k] = 0;
+    bytes[k] = 0.0;
+  }
+  for (int i = 0; i < g_prof_n; ++i) {
+    ProfRec& r = g_prof_recs[i];
+    if (cudaEventSynchronize(r.b) != cudaSuccess) return fail(ADMP_ERR_CUDA, "profile: event sync failed");
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, r.a, r.b) != cudaSuccess) continue;
+    if (r.kernel >= 0 && r.kernel < n) {
+      ms[r.kernel] += t;
+      launches[r.kernel] += 1;
+      bytes[r.kernel] += r.bytes;
+    }
+  }
+  return ADMP_OK;
+}
 
 extern "C" int admp_check_errors(void* stream) {
   bool saved = g_sync;

@@ -21,6 +21,19 @@ bool sync_checks();
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Kernel launch counter (all launches made by this library) and an optional
+// CUDA-event profiler for the hot kernels.  Profiling is off by default; when
+// on, each instrumented launch is bracketed by events on its own stream and
+// tagged with the algorithmic bytes it moves.
+enum ProfKernel {
+  PK_SPREAD = 0, PK_FFT_Z_FWD, PK_FFT_Y_FWD, PK_FFT_X_GREEN, PK_FFT_Y_INV, PK_FFT_Z_INV, PK_GATHER,
+  PK_PAIR_EF, PK_CSR_SPMV, PK_NEIGHBORS, PK_CG_VECTOR, PK_COUNT
+};
+void count_launches(int n);
+bool prof_on();
+int prof_begin(cudaStream_t st);                       // returns a slot (or -1)
+void prof_end(int slot, int kernel, double bytes, cudaStream_t st);
+
 // Carves typed sub-buffers out of a caller workspace.
 struct Carver {
   char* base;

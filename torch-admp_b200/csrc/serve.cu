@@ -1,0 +1,362 @@
+// Batched serving entry points: many independent PME / QEq systems per launch,
+// with per-slot state (positions, CSR neighbour rows, CG vectors and scalars)
+// that persists in caller-owned pools between calls, so a scheduler can admit
+// and retire systems between CG iterations (continuous batching).
+#include "pme_host.h"
+#include "qeq_kernels.cuh"
+#include "serve_kernels.cuh"
+
+namespace admp {
+
+struct SrvLaunch {
+  Batch b;
+  long long pair_off[kMaxBatch];
+  long long pair_cap[kMaxBatch];
+  double rc[kMaxBatch];
+  int cell_off[kMaxBatch];
+};
+
+// (Re)build the per-launch system table; `fresh` recomputes geometry and
+// clears the status (neighbour build), otherwise status comes from slot_info.
+__global__ void srv_table_kernel(SrvLaunch L, const void* box_v, int dbl, const int* __restrict__ slot_info,
+                                 SrvSys* __restrict__ ss, int fresh) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= L.b.nsys) return;
+  const SysDesc& d = L.b.s[s];
+  SrvSys& S = ss[s];
+  S.pair_off = L.pair_off[s];
+  S.pair_cap = L.pair_cap[s];
+  S.rc = L.rc[s];
+  S.kappa = d.kappa;
+  S.kind = d.flags;
+  S.slot = d.box_idx;
+  S.cell_off = L.cell_off[s];
+  if (!fresh) {
+    if (dbl)
+      load_box((const double*)box_v + (size_t)d.box_idx * 9, S.b);
+    else
+      load_box((const float*)box_v + (size_t)d.box_idx * 9, S.b);
+    inv3(S.b, S.bi);
+    S.status = slot_info ? slot_info[4 * d.box_idx + 2] : 0;
+  }
+}
+
+__global__ void slot_export_kernel(Batch b, const CGScal* __restrict__ sc, int* __restrict__ slot_info) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= b.nsys) return;
+  const int sl = b.s[s].box_idx;
+  slot_info[4 * sl + 0] = sc[sl].done;
+  slot_info[4 * sl + 1] = sc[sl].iter;
+  if (sc[sl].status) slot_info[4 * sl + 2] = sc[sl].status;
+}
+
+__global__ void slot_reset_kernel(Batch b, CGScal* __restrict__ sc, int nc) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= b.nsys) return;
+  const int sl = b.s[s].box_idx;
+  CGScal z;
+  memset(&z, 0, sizeof(CGScal));
+  z.n_const = nc;
+  sc[sl] = z;
+}
+
+// zero the CG accumulators of the listed slots, keeping Ginv / b / constants
+__global__ void slot_clear_acc_kernel(Batch b, CGScal* __restrict__ sc) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= b.nsys) return;
+  CGScal& S = sc[b.s[s].box_idx];
+  S.rr = 0.0;
+  S.rr_new = 0.0;
+  S.pHp = 0.0;
+  for (int c = 0; c < kMaxConst; ++c) S.Cv[c] = 0.0;
+  S.sp = 0.0;
+  S.spz = 0.0;
+  S.spz2 = 0.0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) cast_atoms_kernel(Batch b, const T* __restrict__ in, double* __restrict__ out,
+                                                         int to_double, T* __restrict__ back,
+                                                         const double* __restrict__ src) {
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    const int i = d.atom_off + a;
+    if (to_double)
+      out[i] = (double)in[i];
+    else
+      back[i] = (T)src[i];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) zero_vec_kernel(Batch b, T* __restrict__ v) {
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) v[d.atom_off + a] = T(0);
+}
+
+struct SrvCtx {
+  SrvLaunch L;
+  size_t cells_need;
+};
+
+template <typename T>
+static int srv_build(const admp_pools* P, const admp_sys* sys, int nsys, RecipPlan<T>& plan, SrvCtx& c,
+                     bool need_mesh) {
+  if (nsys <= 0 || nsys > kMaxBatch) return fail(ADMP_ERR_BAD_ARG, "serve: %d systems per call (1..%d)", nsys, kMaxBatch);
+  SysSpec spec[kMaxBatch];
+  size_t coff = 0;
+  for (int s = 0; s < nsys; ++s) {
+    const admp_sys& a = sys[s];
+    if (a.natoms <= 0 || a.atom_off < 0 || a.slot < 0) return fail(ADMP_ERR_BAD_ARG, "serve: bad system %d", s);
+    spec[s].natoms = a.natoms;
+    spec[s].atom_off = a.atom_off;
+    for (int d = 0; d < 3; ++d) spec[s].K[d] = a.kmesh[d];
+    spec[s].kappa = a.kappa;
+    spec[s].box_idx = a.slot;
+    c.L.pair_off[s] = a.pair_off;
+    c.L.pair_cap[s] = a.pair_cap;
+    c.L.rc[s] = a.rcut;
+    c.L.cell_off[s] = (int)coff;
+    coff += 3 * (size_t)(2 * a.natoms + 128 + 1);
+  }
+  c.cells_need = coff;
+  int st = build_recip_plan<T>(spec, nsys, plan);
+  if (st) return st;
+  for (int s = 0; s < nsys; ++s) plan.b.s[s].flags = sys[s].kind;
+  c.L.b = plan.b;
+  if (need_mesh) {
+    if ((long long)plan.mesh_elems > P->mesh_cap || (long long)plan.spec_elems > P->spec_cap || nsys > P->acc_cap)
+      return fail(ADMP_ERR_WORKSPACE, "serve: mesh pool too small (need %zu real, %zu complex)", plan.mesh_elems,
+                  plan.spec_elems);
+  }
+  if ((size_t)P->sys_scratch_bytes < sizeof(SrvSys) * nsys) return fail(ADMP_ERR_WORKSPACE, "serve: sys scratch too small");
+  return ADMP_OK;
+}
+
+template <typename T>
+static int serve_neighbors_impl(const admp_pools* P, const admp_sys* sys, int nsys, cudaStream_t st) {
+  RecipPlan<T> plan;
+  SrvCtx c;
+  int s = srv_build<T>(P, sys, nsys, plan, c, false);
+  if (s) return s;
+  if ((long long)c.cells_need > P->cells_cap) return fail(ADMP_ERR_WORKSPACE, "serve: cell pool too small (%zu)", c.cells_need);
+  SrvSys* ss = (SrvSys*)P->sys_scratch;
+  const Batch& b = plan.b;
+  typedef typename Vec4<T>::type V4;
+  srv_table_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(c.L, P->box, sizeof(T) == 8, nullptr, ss, 1);
+  sn_setup_kernel<T><<<nsys, 256, 0, st>>>(b, ss, (const T*)P->box, P->cells);
+  sn_bin_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const T*)P->pos, (V4*)P->frac, P->cell_of, P->cells);
+  sn_scan_cells_kernel<<<nsys, 1024, 0, st>>>(ss, P->cells);
+  sn_scatter_kernel<<<b.nblk_atom, 256, 0, st>>>(b, ss, P->cell_of, P->cells, P->sorted);
+  sn_pairs_kernel<T, false><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, P->cell_of, P->cells, P->sorted,
+                                                         P->pcnt, nullptr, nullptr);
+  sn_scan_rows_kernel<<<nsys, 1024, 0, st>>>(b, ss, P->pcnt, P->pstart, P->slot_info);
+  sn_pairs_kernel<T, true><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, P->cell_of, P->cells, P->sorted,
+                                                        P->pcnt, P->pstart, P->col);
+  count_launches(8);
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
+template <typename T>
+static int serve_ef_impl(const admp_pools* P, const admp_sys* sys, int nsys, double ke, cudaStream_t st) {
+  RecipPlan<T> plan;
+  SrvCtx c;
+  int s = srv_build<T>(P, sys, nsys, plan, c, true);
+  if (s) return s;
+  SrvSys* ss = (SrvSys*)P->sys_scratch;
+  const Batch& b = plan.b;
+  typedef typename Vec4<T>::type V4;
+  srv_table_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(c.L, P->box, sizeof(T) == 8, P->slot_info, ss, 0);
+  zero_atoms_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, (T*)P->force, P->energy);
+  int h = prof_begin(st);
+  pair_ef_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, (const T*)P->q, (const T*)P->eta,
+                                                 P->pstart, P->pcnt, P->col, ke, (T*)P->force, P->energy);
+  prof_end(h, PK_PAIR_EF, plan_atoms(plan) * (sizeof(V4) + 2 * sizeof(T) + 12 + 3 * sizeof(T)), st);
+  count_launches(6);
+  ADMP_CUDA_TRY(cudaMemsetAsync(P->acc, 0, sizeof(double) * kAccStride * nsys, st));
+  s = launch_recip<T>(plan, (const T*)P->pos, (const T*)P->box, (const T*)P->q, (T*)P->mesh, (Cplx<T>*)P->spec,
+                      P->acc, ke, nullptr, (T*)P->force, st);
+  if (s) return s;
+  recip_finalize_kernel<T><<<(nsys + 127) / 128, 128, 0, st>>>(b, (const T*)P->box, P->acc, P->energy, nullptr);
+  sys_terms_kernel<T><<<nsys, 512, 0, st>>>(b, ss, (const T*)P->q, (const T*)P->chi, (const T*)P->hardness,
+                                            (const T*)P->eta, ke, P->energy);
+  negate_atoms_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, (T*)P->force);
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
+// H v for the listed systems: Hv must be zeroed, sums of v in the CG state.
+template <typename T>
+static int srv_matvec(const admp_pools* P, const RecipPlan<T>& plan, QEqParams prm, const T* v, T* Hv,
+                      double* hv_out, double ke, cudaStream_t st) {
+  const Batch& b = plan.b;
+  int s = launch_recip_potential<T>(plan, (const T*)P->pos, (const T*)P->box, v, (T*)P->mesh, (Cplx<T>*)P->spec,
+                                    P->acc, ke, Hv, st);
+  if (s) return s;
+  int h = prof_begin(st);
+  csr_spmv_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->pstart, P->pcnt, P->col, (const T*)P->coef, v, Hv, b.done,
+                                                  b.done_stride);
+  prof_end(h, PK_CSR_SPMV, -1.0, st);
+  count_launches(2);
+  qeq_finish_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, v, Hv, P->cg_diag, P->cg_z, (const T*)nullptr, 0,
+                                                    (CGScal*)P->cg_state, hv_out);
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
+static QEqParams srv_params(double tol, int max_iter, double ke) {
+  QEqParams p;
+  p.flags = ADMP_QEQ_KSPACE | ADMP_QEQ_RSPACE | ADMP_QEQ_DAMPING;
+  p.axis = 2;
+  p.max_iter = max_iter;
+  p.tol = tol;
+  p.ke = ke;
+  return p;
+}
+
+template <typename T>
+static int serve_qeq_init_impl(const admp_pools* P, const admp_sys* sys, int nsys, double tol, int max_iter,
+                               double ke, cudaStream_t st) {
+  RecipPlan<T> plan;
+  SrvCtx c;
+  int s = srv_build<T>(P, sys, nsys, plan, c, true);
+  if (s) return s;
+  SrvSys* ss = (SrvSys*)P->sys_scratch;
+  const Batch& b = plan.b;
+  typedef typename Vec4<T>::type V4;
+  CGScal* sc = (CGScal*)P->cg_state;
+  const QEqParams prm = srv_params(tol, max_iter, ke);
+  srv_table_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(c.L, P->box, sizeof(T) == 8, P->slot_info, ss, 0);
+  slot_reset_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc, 1);
+  qeq_setup_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, (const T*)P->pos, (const T*)P->box, (const T*)P->chi,
+                                                  (const T*)P->hardness, (const T*)P->eta, (const T*)nullptr,
+                                                  P->cg_diag, P->cg_z, P->cg_chi, sc);
+  // total-charge constraint: Gram = N
+  qeq_gram_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, 1, (const T*)nullptr, 0, sc);
+  qeq_gram_invert_kernel<<<(nsys + 31) / 32, 32, 0, st>>>(b, 1, sc);
+  csr_coef_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, (const T*)P->eta, P->pstart, P->pcnt,
+                                                  P->col, ke, (T*)P->coef);
+  // x0 = P(q_warm)
+  cast_atoms_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, (const T*)P->q, P->cg_x, 1, nullptr, nullptr);
+  qeq_sums_kernel<T, double><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_x, P->cg_z, (const T*)nullptr, 0, 1, 1, sc,
+                                                          nullptr, nullptr);
+  qeq_project_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_x, (const T*)nullptr, 0, sc);
+  slot_clear_acc_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc);
+  // H x0
+  qeq_sums_kernel<T, double><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_x, P->cg_z, (const T*)nullptr, 0, 1, 0, sc,
+                                                          (T*)P->cg_hp, (T*)P->cg_p);
+  s = srv_matvec<T>(P, plan, prm, (const T*)P->cg_p, (T*)P->cg_hp, P->cg_hx, ke, st);
+  if (s) return s;
+  slot_clear_acc_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc);
+  zero_vec_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, (T*)P->cg_hp);
+  qeq_resid_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_hx, P->cg_chi, (const T*)nullptr, 0, P->cg_z, P->cg_r,
+                                                   (T*)P->cg_p, sc, 0);
+  qeq_resid_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_hx, P->cg_chi, (const T*)nullptr, 0, P->cg_z, P->cg_r,
+                                                   (T*)P->cg_p, sc, 1);
+  qeq_init_done_kernel<<<(nsys + 31) / 32, 32, 0, st>>>(b, prm, sc);
+  slot_export_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc, P->slot_info);
+  count_launches(18);
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
+template <typename T>
+static int serve_qeq_iterate_impl(const admp_pools* P, const admp_sys* sys, int nsys, int niter, double tol,
+                                  int max_iter, double ke, cudaStream_t st) {
+  RecipPlan<T> plan;
+  SrvCtx c;
+  int s = srv_build<T>(P, sys, nsys, plan, c, true);
+  if (s) return s;
+  CGScal* sc = (CGScal*)P->cg_state;
+  plan.b.done = &sc[0].done;
+  plan.b.done_stride = (int)(sizeof(CGScal) / sizeof(int));
+  const Batch& b = plan.b;
+  const QEqParams prm = srv_params(tol, max_iter, ke);
+  for (int k = 0; k < niter; ++k) {
+    count_launches(3);
+    qeq_rotate_kernel<<<(nsys + 31) / 32, 32, 0, st>>>(b, sc);
+    s = srv_matvec<T>(P, plan, prm, (const T*)P->cg_p, (T*)P->cg_hp, nullptr, ke, st);
+    if (s) return s;
+    qeq_update_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_x, P->cg_r, (const T*)P->cg_p, (T*)P->cg_hp,
+                                                      (const T*)nullptr, 0, sc);
+    qeq_direction_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, P->cg_r, (T*)P->cg_p, P->cg_z, sc);
+  }
+  slot_export_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc, P->slot_info);
+  count_launches(1);
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
+template <typename T>
+static int serve_qeq_finish_impl(const admp_pools* P, const admp_sys* sys, int nsys, cudaStream_t st) {
+  RecipPlan<T> plan;
+  SrvCtx c;
+  int s = srv_build<T>(P, sys, nsys, plan, c, false);
+  if (s) return s;
+  const Batch& b = plan.b;
+  cast_atoms_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, nullptr, nullptr, 0, (T*)P->q, P->cg_x);
+  count_launches(1);
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
+}  // namespace admp
+
+using namespace admp;
+
+extern "C" size_t admp_serve_slot_state_bytes(void) { return sizeof(CGScal); }
+extern "C" size_t admp_serve_sys_scratch_bytes(int nsys) { return sizeof(SrvSys) * (size_t)(nsys > 0 ? nsys : 1); }
+extern "C" size_t admp_serve_cells_needed(const admp_sys* sys, int nsys) {
+  size_t c = 0;
+  for (int s = 0; s < nsys; ++s) c += 3 * (size_t)(2 * sys[s].natoms + 128 + 1);
+  return c;
+}
+
+#define SERVE_DISPATCH(call_f64, call_f32)                   \
+  do {                                                       \
+    if (dtype == ADMP_F64) return call_f64;                  \
+    if (dtype == ADMP_F32) return call_f32;                  \
+    return fail(ADMP_ERR_BAD_ARG, "bad dtype");              \
+  } while (0)
+
+extern "C" int admp_serve_neighbors(int dtype, const admp_pools* P, const admp_sys* sys, int nsys, void* stream) {
+  if (!P || !sys) return fail(ADMP_ERR_BAD_ARG, "serve: null pools/systems");
+  cudaStream_t st = (cudaStream_t)stream;
+  SERVE_DISPATCH(serve_neighbors_impl<double>(P, sys, nsys, st), serve_neighbors_impl<float>(P, sys, nsys, st));
+}
+
+extern "C" int admp_serve_energy_forces(int dtype, const admp_pools* P, const admp_sys* sys, int nsys, double ke,
+                                        void* stream) {
+  if (!P || !sys) return fail(ADMP_ERR_BAD_ARG, "serve: null pools/systems");
+  cudaStream_t st = (cudaStream_t)stream;
+  SERVE_DISPATCH(serve_ef_impl<double>(P, sys, nsys, ke, st), serve_ef_impl<float>(P, sys, nsys, ke, st));
+}
+
+extern "C" int admp_serve_qeq_init(int dtype, const admp_pools* P, const admp_sys* sys, int nsys, double tol,
+                                   int max_iter, double ke, void* stream) {
+  if (!P || !sys) return fail(ADMP_ERR_BAD_ARG, "serve: null pools/systems");
+  cudaStream_t st = (cudaStream_t)stream;
+  SERVE_DISPATCH(serve_qeq_init_impl<double>(P, sys, nsys, tol, max_iter, ke, st),
+                 serve_qeq_init_impl<float>(P, sys, nsys, tol, max_iter, ke, st));
+}
+
+extern "C" int admp_serve_qeq_iterate(int dtype, const admp_pools* P, const admp_sys* sys, int nsys, int niter,
+                                      double tol, int max_iter, double ke, void* stream) {
+  if (!P || !sys || niter < 0) return fail(ADMP_ERR_BAD_ARG, "serve: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  SERVE_DISPATCH(serve_qeq_iterate_impl<double>(P, sys, nsys, niter, tol, max_iter, ke, st),
+                 serve_qeq_iterate_impl<float>(P, sys, nsys, niter, tol, max_iter, ke, st));
+}
+
+extern "C" int admp_serve_qeq_finish(int dtype, const admp_pools* P, const admp_sys* sys, int nsys, void* stream) {
+  if (!P || !sys) return fail(ADMP_ERR_BAD_ARG, "serve: null pools/systems");
+  cudaStream_t st = (cudaStream_t)stream;
+  SERVE_DISPATCH(serve_qeq_finish_impl<double>(P, sys, nsys, st), serve_qeq_finish_impl<float>(P, sys, nsys, st));
+}

@@ -1,0 +1,498 @@
+// Batched kernels of the serving path: many independent systems per launch.
+//
+//   neighbours: per-system cell lists -> CSR rows (pstart, pcnt, col) in a
+//               pair pool at caller-assigned offsets (nblist.py:335-445 set)
+//   pair_ef   : warp per atom over its CSR row: Ewald real space (pme.py:312-349)
+//               and Gaussian damping (qeq.py:104-119) energy, force, potential
+//   csr_coef  : QEq real-space matrix entries ke (erfc(kappa r) - erfc(r / 2 eta_ij)) / r
+//   csr_spmv  : Hp += J_real p, warp per row
+//   sys_terms : per-system self / non-neutral / damping-self / site energies
+#pragma once
+
+#include "pme_kernels.cuh"
+
+namespace admp {
+
+struct SrvSys {          // per-system data of one launch (device array)
+  double b[9], bi[9];
+  int nc[3];
+  int ncells;
+  int cell_off;          // into the cell scratch
+  int status;
+  long long pair_off, pair_cap, pair_need;
+  double rc, kappa;
+  int kind;              // 0 PME, 1 QEq
+  int slot;
+};
+
+template <typename T>
+struct Vec4 {
+  typedef float4 type;
+};
+template <>
+struct Vec4<double> {
+  typedef double4 type;
+};
+
+__device__ __forceinline__ double4 mk4(double a, double b, double c, double d) { return make_double4(a, b, c, d); }
+__device__ __forceinline__ float4 mk4f(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+
+template <typename T>
+__device__ __forceinline__ typename Vec4<T>::type make_v4(T a, T b, T c, T d);
+template <>
+__device__ __forceinline__ float4 make_v4<float>(float a, float b, float c, float d) {
+  return make_float4(a, b, c, d);
+}
+template <>
+__device__ __forceinline__ double4 make_v4<double>(double a, double b, double c, double d) {
+  return make_double4(a, b, c, d);
+}
+
+// one block per system: geometry, grid, zero the cell counters
+template <typename T>
+__global__ void sn_setup_kernel(Batch b, SrvSys* __restrict__ ss, const T* __restrict__ box, int* __restrict__ cells) {
+  const int s = blockIdx.x;
+  SrvSys& S = ss[s];
+  __shared__ int nc_sh[4];
+  if (threadIdx.x == 0) {
+    load_box(box + (size_t)b.s[s].box_idx * 9, S.b);
+    const double V = inv3(S.b, S.bi);
+    double h[3];
+    for (int d = 0; d < 3; ++d) {
+      const double* u = S.b + ((d + 1) % 3) * 3;
+      const double* v = S.b + ((d + 2) % 3) * 3;
+      const double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2], cz = u[0] * v[1] - u[1] * v[0];
+      h[d] = fabs(V) / sqrt(cx * cx + cy * cy + cz * cz);
+    }
+    S.status = 0;
+    S.pair_need = 0;
+    if (!(S.rc <= fmin(h[0], fmin(h[1], h[2])) / 2.0)) S.status = ADMP_ERR_CUTOFF_TOO_LARGE;
+    if (!isfinite(V) || V == 0.0) S.status = ADMP_ERR_NONFINITE;
+    const int cap = 2 * b.s[s].natoms + 128;
+    int nc[3];
+    for (int d = 0; d < 3; ++d) {
+      const double r = h[d] / S.rc;
+      nc[d] = (r >= 1.0 && r < 1e6) ? (int)floor(r) : 1;
+    }
+    while ((long long)nc[0] * nc[1] * nc[2] > cap) {
+      const int d = nc[0] >= nc[1] && nc[0] >= nc[2] ? 0 : (nc[1] >= nc[2] ? 1 : 2);
+      nc[d] = (nc[d] + 1) / 2;
+    }
+    for (int d = 0; d < 3; ++d) S.nc[d] = nc[d];
+    S.ncells = nc[0] * nc[1] * nc[2];
+    nc_sh[0] = S.ncells;
+  }
+  __syncthreads();
+  int* cnt = cells + S.cell_off;
+  const int n = 3 * (nc_sh[0] + 1);
+  for (int k = threadIdx.x; k < n; k += blockDim.x) cnt[k] = 0;
+}
+
+template <typename T>
+static __global__ void __launch_bounds__(256)
+    sn_bin_kernel(Batch b, SrvSys* __restrict__ ss, const T* __restrict__ pos, typename Vec4<T>::type* __restrict__ frac,
+                  int* __restrict__ cell_of, int* __restrict__ cells) {
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const SrvSys& S = ss[s];
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    const int i = d.atom_off + a;
+    if (S.status) {
+      cell_of[i] = -1;
+      continue;
+    }
+    const double r0 = pos[3 * (size_t)i], r1 = pos[3 * (size_t)i + 1], r2 = pos[3 * (size_t)i + 2];
+    double f[3];
+    int c[3];
+    bool ok = isfinite(r0) && isfinite(r1) && isfinite(r2);
+    for (int e = 0; e < 3; ++e) {
+      f[e] = r0 * S.bi[0 * 3 + e] + r1 * S.bi[1 * 3 + e] + r2 * S.bi[2 * 3 + e];
+      f[e] -= floor(f[e]);
+      c[e] = ok ? min((int)(f[e] * S.nc[e]), S.nc[e] - 1) : 0;
+    }
+    frac[i] = make_v4<T>((T)f[0], (T)f[1], (T)f[2], T(0));
+    if (!ok) {
+      cell_of[i] = -1;
+      continue;
+    }
+    const int id = (c[0] * S.nc[1] + c[1]) * S.nc[2] + c[2];
+    cell_of[i] = id;
+    atomicAdd(cells + S.cell_off + id, 1);
+  }
+}
+
+// block per system: exclusive scan of the cell counts -> starts
+static __global__ void sn_scan_cells_kernel(SrvSys* __restrict__ ss, int* __restrict__ cells) {
+  __shared__ int part[1024];
+  const SrvSys& S = ss[blockIdx.x];
+  const int n = S.ncells;
+  int* cnt = cells + S.cell_off;
+  int* start = cnt + (n + 1);
+  const int nt = blockDim.x, chunk = (n + nt - 1) / nt;
+  const int b0 = threadIdx.x * chunk, b1 = min(b0 + chunk, n);
+  int acc = 0;
+  for (int i = b0; i < b1; ++i) acc += cnt[i];
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int k = 0; k < nt; ++k) {
+      const int v = part[k];
+      part[k] = t;
+      t += v;
+    }
+    start[n] = t;
+  }
+  __syncthreads();
+  acc = part[threadIdx.x];
+  for (int i = b0; i < b1; ++i) {
+    start[i] = acc;
+    acc += cnt[i];
+  }
+}
+
+static __global__ void __launch_bounds__(256)
+    sn_scatter_kernel(Batch b, const SrvSys* __restrict__ ss, const int* __restrict__ cell_of, int* __restrict__ cells,
+                      int* __restrict__ sorted) {
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const SrvSys& S = ss[s];
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  const int n = S.ncells;
+  const int* start = cells + S.cell_off + (n + 1);
+  int* cursor = cells + S.cell_off + 2 * (n + 1);
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    const int i = d.atom_off + a;
+    const int c = cell_of[i];
+    if (c < 0) continue;
+    sorted[d.atom_off + start[c] + atomicAdd(cursor + c, 1)] = i;
+  }
+}
+
+__device__ __forceinline__ void sn_offsets(int nc, int* off, int& n) {
+  if (nc >= 3) {
+    off[0] = -1; off[1] = 0; off[2] = 1; n = 3;
+  } else if (nc == 2) {
+    off[0] = 0; off[1] = 1; n = 2;
+  } else {
+    off[0] = 0; n = 1;
+  }
+}
+
+// thread per atom; COUNT: pcnt[i]; FILL: col[pstart[i] + k]
+template <typename T, bool FILL>
+static __global__ void __launch_bounds__(256)
+    sn_pairs_kernel(Batch b, const SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
+                    const int* __restrict__ cell_of, const int* __restrict__ cells, const int* __restrict__ sorted,
+                    int* __restrict__ pcnt, const long long* __restrict__ pstart, int* __restrict__ col) {
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const SrvSys& S = ss[s];
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  if (FILL && S.status) return;
+  const int n = S.ncells;
+  const int* start = cells + S.cell_off + (n + 1);
+  const double rc2 = S.rc * S.rc;
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    const int i = d.atom_off + a;
+    const int ci = S.status ? -1 : cell_of[i];
+    if (ci < 0) {
+      if (!FILL) pcnt[i] = 0;
+      continue;
+    }
+    const int nc0 = S.nc[0], nc1 = S.nc[1], nc2 = S.nc[2];
+    const int c0 = ci / (nc1 * nc2), c1 = (ci / nc2) % nc1, c2 = ci % nc2;
+    int o0[3], o1[3], o2[3], n0, n1, n2;
+    sn_offsets(nc0, o0, n0);
+    sn_offsets(nc1, o1, n1);
+    sn_offsets(nc2, o2, n2);
+    const typename Vec4<T>::type fi = frac[i];
+    int cnt = 0;
+    const long long base = FILL ? pstart[i] : 0;
+    for (int ia = 0; ia < n0; ++ia) {
+      const int x = (c0 + o0[ia] + nc0) % nc0;
+      for (int ib = 0; ib < n1; ++ib) {
+        const int y = (c1 + o1[ib] + nc1) % nc1;
+        for (int ic = 0; ic < n2; ++ic) {
+          const int z = (c2 + o2[ic] + nc2) % nc2;
+          const int cc = (x * nc1 + y) * nc2 + z;
+          for (int t = start[cc]; t < start[cc + 1]; ++t) {
+            const int j = sorted[d.atom_off + t];
+            if (j == i) continue;
+            const typename Vec4<T>::type fj = frac[j];
+            double df[3] = {(double)fj.x - (double)fi.x, (double)fj.y - (double)fi.y, (double)fj.z - (double)fi.z};
+            for (int e = 0; e < 3; ++e) df[e] -= floor(df[e] + 0.5);
+            double r2 = 0.0;
+            for (int e = 0; e < 3; ++e) {
+              const double v = df[0] * S.b[0 * 3 + e] + df[1] * S.b[1 * 3 + e] + df[2] * S.b[2 * 3 + e];
+              r2 += v * v;
+            }
+            if (r2 < rc2 && r2 > 1e-4) {
+              if (FILL) col[base + cnt] = j;
+              ++cnt;
+            }
+          }
+        }
+      }
+    }
+    if (!FILL) pcnt[i] = cnt;
+  }
+}
+
+// block per system: row starts pstart = pair_off + exclusive prefix; capacity check
+static __global__ void sn_scan_rows_kernel(Batch b, SrvSys* __restrict__ ss, const int* __restrict__ pcnt,
+                                    long long* __restrict__ pstart, int* __restrict__ slot_info) {
+  __shared__ long long part[1024];
+  const SysDesc& d = b.s[blockIdx.x];
+  SrvSys& S = ss[blockIdx.x];
+  const int n = d.natoms;
+  const int nt = blockDim.x, chunk = (n + nt - 1) / nt;
+  const int b0 = threadIdx.x * chunk, b1 = min(b0 + chunk, n);
+  long long acc = 0;
+  for (int a = b0; a < b1; ++a) acc += pcnt[d.atom_off + a];
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int k = 0; k < nt; ++k) {
+      const long long v = part[k];
+      part[k] = t;
+      t += v;
+    }
+    S.pair_need = t;
+    if (!S.status && t > S.pair_cap) S.status = ADMP_ERR_CAPACITY;
+    if (slot_info) {
+      int* si = slot_info + 4 * d.box_idx;
+      si[2] = S.status;
+      si[3] = (int)(t < 2147483647LL ? t : 2147483647LL);
+    }
+  }
+  __syncthreads();
+  acc = S.pair_off + part[threadIdx.x];
+  for (int a = b0; a < b1; ++a) {
+    pstart[d.atom_off + a] = acc;
+    acc += pcnt[d.atom_off + a];
+  }
+}
+
+// minimum-image Cartesian displacement r_j - r_i from wrapped fractional coords
+template <typename V4>
+__device__ __forceinline__ void disp(const V4& fi, const V4& fj, const double* bx, float* dr) {
+  float df[3] = {fj.x - fi.x, fj.y - fi.y, fj.z - fi.z};
+#pragma unroll
+  for (int e = 0; e < 3; ++e) df[e] -= floorf(df[e] + 0.5f);
+#pragma unroll
+  for (int e = 0; e < 3; ++e) dr[e] = df[0] * (float)bx[e] + df[1] * (float)bx[3 + e] + df[2] * (float)bx[6 + e];
+}
+template <typename V4>
+__device__ __forceinline__ void disp(const V4& fi, const V4& fj, const double* bx, double* dr) {
+  double df[3] = {fj.x - fi.x, fj.y - fi.y, fj.z - fi.z};
+#pragma unroll
+  for (int e = 0; e < 3; ++e) df[e] -= floor(df[e] + 0.5);
+#pragma unroll
+  for (int e = 0; e < 3; ++e) dr[e] = df[0] * bx[e] + df[1] * bx[3 + e] + df[2] * bx[6 + e];
+}
+
+// warp per atom: real-space Ewald (+ damping for QEq systems) energy, gradient, potential
+template <typename T>
+static __global__ void __launch_bounds__(256)
+    pair_ef_kernel(Batch b, const SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
+                   const T* __restrict__ q, const T* __restrict__ eta, const long long* __restrict__ pstart,
+                   const int* __restrict__ pcnt, const int* __restrict__ col, double ke, T* __restrict__ grad,
+                   double* __restrict__ energy) {
+  __shared__ double bx[9];
+  __shared__ double red[32];
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const SrvSys& S = ss[s];
+  if (threadIdx.x < 9) bx[threadIdx.x] = S.b[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  const T kappa = (T)S.kappa, kt = (T)ke;
+  const T tsp = T(2.0 / kSqrtPi);
+  const bool damp = S.kind == 1 && eta != nullptr;
+  double e_acc = 0.0;
+  if (!S.status) {
+    for (int a = a0 + warp; a < a1; a += blockDim.x >> 5) {
+      const int i = d.atom_off + a;
+      const typename Vec4<T>::type fi = frac[i];
+      const T qi = q[i];
+      const T ei = damp ? eta[i] : T(0);
+      const long long st = pstart[i];
+      const int n = pcnt[i];
+      T g0 = 0, g1 = 0, g2 = 0, e = 0;
+      for (int k = lane; k < n; k += 32) {
+        const int j = col[st + k];
+        const typename Vec4<T>::type fj = frac[j];
+        T dr[3];
+        disp(fi, fj, bx, dr);
+        const T r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+        const T r = sqrt_t(r2);
+        const T inv = T(1) / r;
+        const T qq = qi * q[j] * kt;
+        const T x = kappa * r;
+        const T er = erfc_t(x);
+        T ep = er * inv;
+        T dd = -tsp * kappa * exp_t(-x * x) * inv - er * inv * inv;
+        if (damp) {
+          const T ej = eta[j];
+          T eij = sqrt_t((ei * ei + ej * ej) * T(0.5));
+          if (eij == T(0)) eij = T(1e-10);
+          const T y = r / (T(2) * eij);
+          const T ed = erfc_t(y);
+          ep -= ed * inv;
+          dd += tsp * exp_t(-y * y) / (T(2) * eij) * inv + ed * inv * inv;
+        }
+        e += qq * ep;
+        // dE/dr_i = dE/dr * d r / d r_i = dd * qq * (-(r_j - r_i) / r)
+        const T gs = -dd * qq * inv;
+        g0 += gs * dr[0];
+        g1 += gs * dr[1];
+        g2 += gs * dr[2];
+      }
+      e = warp_sum(e);
+      g0 = warp_sum(g0);
+      g1 = warp_sum(g1);
+      g2 = warp_sum(g2);
+      if (lane == 0) {
+        grad[3 * (size_t)i] += g0;
+        grad[3 * (size_t)i + 1] += g1;
+        grad[3 * (size_t)i + 2] += g2;
+        e_acc += 0.5 * (double)e;  // each pair appears in both rows
+      }
+    }
+  }
+  double v[1] = {e_acc};
+  block_atomic_sum<1>(v, energy + d.box_idx, red);
+}
+
+// QEq real-space matrix entries (CSR)
+template <typename T>
+static __global__ void __launch_bounds__(256)
+    csr_coef_kernel(Batch b, const SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
+                    const T* __restrict__ eta, const long long* __restrict__ pstart, const int* __restrict__ pcnt,
+                    const int* __restrict__ col, double ke, T* __restrict__ coef) {
+  __shared__ double bx[9];
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const SrvSys& S = ss[s];
+  if (threadIdx.x < 9) bx[threadIdx.x] = S.b[threadIdx.x];
+  __syncthreads();
+  if (S.status) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  const T kappa = (T)S.kappa;
+  for (int a = a0 + warp; a < a1; a += blockDim.x >> 5) {
+    const int i = d.atom_off + a;
+    const typename Vec4<T>::type fi = frac[i];
+    const T ei = eta[i];
+    const long long st = pstart[i];
+    const int n = pcnt[i];
+    for (int k = lane; k < n; k += 32) {
+      const int j = col[st + k];
+      T dr[3];
+      disp(fi, frac[j], bx, dr);
+      const T r = sqrt_t(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      const T ej = eta[j];
+      T eij = sqrt_t((ei * ei + ej * ej) * T(0.5));
+      if (eij == T(0)) eij = T(1e-10);
+      coef[st + k] = (T)ke * (erfc_t(kappa * r) - erfc_t(r / (T(2) * eij))) / r;
+    }
+  }
+}
+
+// Hp[i] += sum_k coef[k] p[col[k]]  (warp per row)
+template <typename T>
+static __global__ void __launch_bounds__(256)
+    csr_spmv_kernel(Batch b, const long long* __restrict__ pstart, const int* __restrict__ pcnt,
+                    const int* __restrict__ col, const T* __restrict__ coef, const T* __restrict__ p,
+                    T* __restrict__ Hp, const int* __restrict__ done, int done_stride) {
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  if (done && done[(size_t)d.box_idx * done_stride]) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  for (int a = a0 + warp; a < a1; a += blockDim.x >> 5) {
+    const int i = d.atom_off + a;
+    const long long st = pstart[i];
+    const int n = pcnt[i];
+    T acc = 0;
+    for (int k = lane; k < n; k += 32) acc += coef[st + k] * p[col[st + k]];
+    acc = warp_sum(acc);
+    if (lane == 0) Hp[i] += acc;
+  }
+}
+
+// block per system: self + non-neutral (+ damping self + site for QEq systems)
+template <typename T>
+__global__ void __launch_bounds__(512)
+    sys_terms_kernel(Batch b, const SrvSys* __restrict__ ss, const T* __restrict__ q, const T* __restrict__ chi,
+                     const T* __restrict__ hard, const T* __restrict__ eta, double ke, double* __restrict__ energy) {
+  __shared__ double red[4 * 32];
+  __shared__ double sums[4];
+  const SysDesc& d = b.s[blockIdx.x];
+  const SrvSys& S = ss[blockIdx.x];
+  if (threadIdx.x < 4) sums[threadIdx.x] = 0.0;
+  __syncthreads();
+  const bool qeq = S.kind == 1;
+  double v[4] = {0, 0, 0, 0};
+  for (int a = threadIdx.x; a < d.natoms; a += blockDim.x) {
+    const int i = d.atom_off + a;
+    const double qi = q[i];
+    v[0] += qi;
+    v[1] += qi * qi;
+    if (qeq) {
+      const double e = eta[i];
+      v[2] += (fabs(e) > 1e-4 ? 1.0 / e : 0.0) / (2.0 * kSqrtPi) * qi * qi;
+      v[3] += (double)chi[i] * qi + (double)hard[i] * qi * qi;
+    }
+  }
+  block_atomic_sum<4>(v, sums, red);
+  if (threadIdx.x == 0) {
+    const double V = fabs(S.b[0] * (S.b[4] * S.b[8] - S.b[5] * S.b[7]) - S.b[1] * (S.b[3] * S.b[8] - S.b[5] * S.b[6]) +
+                          S.b[2] * (S.b[3] * S.b[7] - S.b[4] * S.b[6]));
+    const double kap = S.kappa;
+    double E = -ke * kap / kSqrtPi * sums[1] - kPi / (2.0 * V * kap * kap) * ke * sums[0] * sums[0];
+    if (qeq) E += ke * sums[2] + sums[3];
+    energy[d.box_idx] += E;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) zero_atoms_kernel(Batch b, T* __restrict__ a3, double* __restrict__ energy) {
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    const size_t i = (size_t)(d.atom_off + a);
+    a3[3 * i] = T(0);
+    a3[3 * i + 1] = T(0);
+    a3[3 * i + 2] = T(0);
+  }
+  if (threadIdx.x == 0 && blockIdx.x == d.blk_atom) energy[d.box_idx] = 0.0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) negate_atoms_kernel(Batch b, T* __restrict__ a3) {
+  const int s = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    const size_t i = (size_t)(d.atom_off + a);
+    a3[3 * i] = -a3[3 * i];
+    a3[3 * i + 1] = -a3[3 * i + 1];
+    a3[3 * i + 2] = -a3[3 * i + 2];
+  }
+}
+
+}  // namespace admp

@@ -98,6 +98,22 @@ int admp_pme_recip(int dtype, int nframes, int natoms, const int* kmesh, const v
                    void* dE_dpos, void* dE_dq, void* dE_dbox, void* workspace,
                    size_t workspace_bytes, void* stream);
 
+/* Variant of admp_pme_recip that allocates nothing and takes no workspace,  */
+/* for callers that cannot allocate device memory when they call (e.g. a    */
+/* plugin inside an MD engine that owns all device memory, or a step loop   */
+/* that must not trigger cudaMalloc's device-wide synchronisation).  It has */
+/* no counterpart in the reference.  Its scratch is a fixed 16 MiB array in */
+/* the library's device memory (admp_pme_recip_noalloc_max_scratch()), held */
+/* by every GPU that loads the library until exit; calls needing more       */
+/* scratch than that (admp_pme_recip_workspace_size) return               */
+/* ADMP_ERR_WORKSPACE.  The first call on a device looks up the array's     */
+/* device address (cudaGetSymbolAddress) and should come before any stream */
+/* capture.  All calls share the array: calls that overlap on the GPU race. */
+size_t admp_pme_recip_noalloc_max_scratch(void);
+int admp_pme_recip_noalloc(int dtype, int nframes, int natoms, const int* kmesh, const void* pos,
+                           const void* box, const void* q, double kappa, double ke, double* energy,
+                           void* dE_dpos, void* dE_dq, void* dE_dbox, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Pair terms over a caller pair list.                                       */
 /* Replaces _forward_pbc_real (pme.py:312-349), _forward_obc (pme.py:529-561) */

@@ -28,7 +28,8 @@ EXPORTS = [
     "admp_nblist_count", "admp_nblist_fill", "admp_qeq_workspace_size", "admp_qeq_solve", "admp_qeq_hvp",
     "admp_launch_count", "admp_profile_enable", "admp_profile_read", "admp_serve_slot_state_bytes",
     "admp_serve_sys_scratch_bytes", "admp_serve_cells_needed", "admp_serve_neighbors", "admp_serve_energy_forces",
-    "admp_serve_qeq_init", "admp_serve_qeq_iterate", "admp_serve_qeq_finish",
+    "admp_serve_qeq_init", "admp_serve_qeq_iterate", "admp_serve_qeq_finish", "admp_pme_recip_noalloc_max_scratch",
+    "admp_pme_recip_noalloc",
 ]
 PROFILE_KERNELS = ["spread", "fft_z_fwd", "fft_y_fwd", "fft_x_green", "fft_y_inv", "fft_z_inv", "gather", "pair_ef",
                    "csr_spmv", "neighbors", "cg_vector"]
@@ -60,6 +61,8 @@ _SIGS = {
     "admp_qeq_hvp": (_i, [_i, _i, _i, _ip, _vp, _vp, _ll, _vp, _vp, _vp, _vp, _vp, _d, _d, _vp, _vp, _vp, _sz,
                           _vp]),
     "admp_launch_count": (_ll, []),
+    "admp_pme_recip_noalloc_max_scratch": (_sz, []),
+    "admp_pme_recip_noalloc": (_i, [_i, _i, _i, _ip, _vp, _vp, _vp, _d, _d, _vp, _vp, _vp, _vp, _vp]),
     "admp_profile_enable": (_i, [_i]),
     "admp_profile_read": (_i, [_dp, _llp, _dp, _i]),
 }

@@ -67,8 +67,11 @@ def rank_info():
 
 # ---------------------------------------------------------------- CPU oracle
 def _cpu_one(req_tuple):
-    """One request on the CPU oracle (restatement of the reference path)."""
+    """One request on the CPU oracle (restatement of the reference path:
+    cell-list neighbours, PME energy + forces, or the reference's projected
+    nonlinear CG for QEq followed by energy + forces).  Returns seconds."""
     from oracle import admp_oracle as O
+    t0 = time.perf_counter()
     kind, pos, box, q, chi, hard, eta = req_tuple
     kappa = O.ewald_kappa(RCUT, ETHRESH)
     km = O.auto_kmesh(box, kappa, ETHRESH)
@@ -76,39 +79,53 @@ def _cpu_one(req_tuple):
     bs = O.pair_buffer_scales(pairs)
     if kind == "pme":
         O.coulomb_forces(pos, box, pairs, bs, q, rcut=RCUT, ethresh=ETHRESH, kmesh=km)
-        return 1
+        return time.perf_counter() - t0
     ds = O.pairs_ds(pos, pairs, box)
     s = O.QEqSystem(pos, box, chi, hard, eta, pairs, ds, bs, rcut=RCUT, ethresh=ETHRESH, kmesh=km)
     n = pos.shape[0]
     qs, _ = O.solve_quadratic(s, np.zeros(n), np.ones((1, n)), np.zeros(1), max_iter=200, eps=TOL)
     O.coulomb_forces(pos, box, pairs, bs, qs, rcut=RCUT, ethresh=ETHRESH, kmesh=km)
-    return 1
+    return time.perf_counter() - t0
+
+
+CPU_SAMPLE_SIZES = {"pme": (300, 1000, 3000, 6000), "qeq": (300, 900, 2400)}
 
 
 def cpu_baseline(stream, seconds: float):
-    """Serve requests of the stream on all host cores (spawn pool, one request
-    per task) for about `seconds`; returns (systems/s, cores, sample text)."""
+    """CPU oracle throughput on the stream, from a timed sample.
+
+    Requests of each kind closest to the sizes in CPU_SAMPLE_SIZES are run
+    one per process on the host cores (spawn pool); a power law t = a N^b
+    fitted per kind to their single-core times predicts every request of the
+    stream, and the stream throughput is cores / mean(predicted time) (the
+    requests are independent, so they spread over the cores).  Returns
+    (systems/s, cores, sample text)."""
     import multiprocessing as mp
     cores = os.cpu_count() or 1
+    picks = []
+    for kind, sizes in CPU_SAMPLE_SIZES.items():
+        cand = [r for r in stream if r.kind == kind]
+        for n in sizes:
+            if cand:
+                picks.append(min(cand, key=lambda r: abs(r.natoms - n)))
+    tasks = [(r.kind, r.pos, r.box, r.charges, r.chi, r.hardness, r.eta) for r in picks]
     ctx = mp.get_context("spawn")
-    tasks = [(r.kind, r.pos, r.box, r.charges, r.chi, r.hardness, r.eta) for r in stream]
-    done = 0
-    atoms = 0
     t0 = time.perf_counter()
-    with ctx.Pool(cores) as pool:
-        it = pool.imap(_cpu_one, tasks, chunksize=1)
-        for k in range(len(tasks)):
-            try:
-                it.next(timeout=max(1.0, seconds * 4))
-            except Exception:
-                break
-            done += 1
-            atoms += stream[k].natoms
-            if time.perf_counter() - t0 > seconds:
-                break
-        el = time.perf_counter() - t0
-        pool.terminate()
-    return done / el, cores, f"first {done} requests of the stream ({atoms} atoms) in {el:.1f} s"
+    with ctx.Pool(min(cores, len(tasks))) as pool:
+        times = pool.map(_cpu_one, tasks, chunksize=1)
+    wall = time.perf_counter() - t0
+    pred = 0.0
+    for kind in CPU_SAMPLE_SIZES:
+        pts = [(r.natoms, t) for r, t in zip(picks, times) if r.kind == kind]
+        x = np.log([p[0] for p in pts])
+        y = np.log([p[1] for p in pts])
+        b, a = np.polyfit(x, y, 1) if len(pts) > 1 else (1.0, y[0] - x[0])
+        pred += sum(math.exp(a + b * math.log(r.natoms)) for r in stream if r.kind == kind)
+    value = cores * len(stream) / pred
+    desc = (f"{len(picks)} requests timed single-core ({', '.join(f'{r.kind} {r.natoms}: {t:.2f}s' for r, t in zip(picks, times))}; "
+            f"wall {wall:.1f}s), power-law fit per kind extrapolated to all {len(stream)} requests "
+            f"(predicted {pred:.0f} core-seconds)")
+    return value, cores, desc
 
 
 # ---------------------------------------------------------------- GPU helpers
@@ -171,8 +188,9 @@ def to_device_requests(stream, dev, dtype):
     out = []
     for r in stream:
         c = copy.copy(r)
-        c.pos = torch.as_tensor(r.pos, dtype=dtype, device=dev)
-        c.box = r.box
+        c.pos = torch.as_tensor(r.pos, dtype=torch.float64, device=dev)
+        c.box_host = r.box
+        c.box = torch.as_tensor(r.box, dtype=torch.float64, device=dev)
         if r.kind == "pme":
             c.charges = torch.as_tensor(r.charges, dtype=dtype, device=dev)
         else:
@@ -261,9 +279,13 @@ def main():
     stream = synthetic.serving_stream(args.nreq, SEED + rank, RATE)
     total_atoms = sum(r.natoms for r in stream)
     dstream = to_device_requests(stream, dev, torch.float32)
-    eng = ServingEngine(device=dev, dtype=torch.float32, max_atoms=6_000_000, max_slots=1024,
-                        mesh_budget=96_000_000, rcut=RCUT, ethresh=ETHRESH, tol=TOL, max_iter=300,
-                        iters_per_tick=8)
+    # pools sized to the stream (capped): all requests fit, so admission never stalls the closed loop
+    from admp_b200.serving import auto_kmesh
+    kap = math.sqrt(-math.log(2 * ETHRESH)) / RCUT
+    mesh_sum = sum(int(np.prod(auto_kmesh(np.diagonal(r.box), kap, ETHRESH))) for r in stream)
+    eng = ServingEngine(device=dev, dtype=torch.float32, max_atoms=min(6_000_000, int(total_atoms * 1.1) + 65536),
+                        max_slots=min(1024, args.nreq + 8), mesh_budget=min(96_000_000, mesh_sum + 4_000_000),
+                        rcut=RCUT, ethresh=ETHRESH, tol=TOL, max_iter=300, iters_per_tick=8)
 
     def one_pass(reqs, to_host=True, arrivals=False, rate_scale=1.0):
         eng.results = []

@@ -264,6 +264,11 @@ typedef struct admp_pools {
   double* acc;         int acc_cap;          /* systems (32 doubles each) */
   int* cells;          long long cells_cap;  /* ints */
   void* sys_scratch;   long long sys_scratch_bytes;
+  /* optional double copies used only for the neighbour decisions of FP32
+   * pools (which pairs lie inside rc), so the pair set equals the FP64 one */
+  double* pos64;       /* [A,3] or NULL */
+  double* box64;       /* [S,3,3] or NULL */
+  void* frac64;        /* [A] double4 scratch, needed with pos64 */
 } admp_pools;
 
 size_t admp_serve_slot_state_bytes(void);

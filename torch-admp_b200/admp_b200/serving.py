@@ -54,7 +54,7 @@ class AdmpPools(ctypes.Structure):
                                   "cg_diag", "cg_z", "cg_chi", "cg_hx", "cg_p", "cg_hp", "mesh")] + \
                [("mesh_cap", ctypes.c_longlong), ("spec", _P), ("spec_cap", ctypes.c_longlong), ("acc", _P),
                 ("acc_cap", ctypes.c_int), ("cells", _P), ("cells_cap", ctypes.c_longlong), ("sys_scratch", _P),
-                ("sys_scratch_bytes", ctypes.c_longlong)]
+                ("sys_scratch_bytes", ctypes.c_longlong), ("pos64", _P), ("box64", _P), ("frac64", _P)]
 
 
 def _bind_serve(lib):
@@ -186,12 +186,19 @@ class ServingEngine:
             "sys_scratch": torch.zeros(self.lib.admp_serve_sys_scratch_bytes(MAX_PER_LAUNCH), dtype=torch.uint8,
                                        device=self.dev),
         }
+        if dtype == torch.float32:
+            # double copies for the neighbour decisions: the FP32 pair set equals the FP64 one
+            self.t["pos64"] = torch.zeros(A, 3, **f64)
+            self.t["box64"] = torch.zeros(max_slots, 3, 3, **f64)
+            self.t["frac64"] = torch.zeros(A, 4, **f64)
         t = self.t
         self.pools = AdmpPools()
         for name in ("pos", "q", "chi", "hardness", "eta", "force", "frac", "pstart", "pcnt", "cell_of", "sorted",
                      "col", "coef", "box", "energy", "cg_state", "slot_info", "cg_x", "cg_r", "cg_diag", "cg_z",
                      "cg_chi", "cg_hx", "cg_p", "cg_hp", "mesh", "spec", "acc", "cells", "sys_scratch"):
             setattr(self.pools, name, t[name].data_ptr())
+        for name in ("pos64", "box64", "frac64"):
+            setattr(self.pools, name, t[name].data_ptr() if name in t else None)
         self.pools.mesh_cap = mesh_budget
         self.pools.spec_cap = mesh_budget + 1024
         self.pools.acc_cap = MAX_PER_LAUNCH
@@ -212,9 +219,13 @@ class ServingEngine:
         self.results_to_host = True
 
     # -- resources -----------------------------------------------------------
+    @staticmethod
+    def _box_host(req):
+        return np.asarray(getattr(req, "box_host", None) if getattr(req, "box_host", None) is not None else req.box)
+
     def _pair_estimate(self, req) -> int:
         n = req.natoms
-        V = abs(float(np.linalg.det(req.box)))
+        V = abs(float(np.linalg.det(self._box_host(req))))
         rho = n / V
         mean = rho * 4.0 / 3.0 * math.pi * self.rcut ** 3
         return int(n * (mean * 1.35 + 24)) + 256
@@ -227,7 +238,7 @@ class ServingEngine:
         fb = 4 if self.dtype == torch.float32 else 8
         per_atom = fb * 17 + 8 * 7 + 4 * 3
         per_pair = 4 + fb
-        km = auto_kmesh(np.diagonal(req.box), self.kappa, self.ethresh)
+        km = auto_kmesh(np.diagonal(self._box_host(req)), self.kappa, self.ethresh)
         return {"atom_bytes": req.natoms * per_atom, "pair_bytes": self._pair_estimate(req) * per_pair,
                 "mesh_elems": self._mesh_of(km)}
 
@@ -281,7 +292,7 @@ class ServingEngine:
                 keep.append((req, tarr))
                 continue
             n = req.natoms
-            km = auto_kmesh(np.diagonal(req.box), self.kappa, self.ethresh)
+            km = auto_kmesh(np.diagonal(self._box_host(req)), self.kappa, self.ethresh)
             m = self._mesh_of(km)
             if not self.free_slots or m > self.mesh_budget:
                 keep.append((req, tarr))
@@ -314,6 +325,12 @@ class ServingEngine:
         t = torch.from_numpy(np.ascontiguousarray(x, dtype=npdt)).pin_memory()
         return t, t.numel() * t.element_size()
 
+    def _src64(self, x):
+        if isinstance(x, torch.Tensor):
+            return x.to(torch.float64), 0
+        t = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).pin_memory()
+        return t, t.numel() * t.element_size()
+
     def _upload(self, items: List[_Active]) -> None:
         t = self.t
         npdt = np.float32 if self.dtype == torch.float32 else np.float64
@@ -321,10 +338,19 @@ class ServingEngine:
             r = a.req
             n = r.natoms
             sl = slice(a.atom_off, a.atom_off + n)
-            pos, nb = self._src(r.pos, npdt)
-            t["pos"][sl].copy_(pos.reshape(n, 3), non_blocking=True)
-            bx, b2 = self._src(r.box, npdt)
-            t["box"][a.slot].copy_(bx.reshape(3, 3), non_blocking=True)
+            if "pos64" in t:
+                # positions and box arrive in double; the FP32 copies are made on the device
+                p64, nb = self._src64(r.pos)
+                t["pos64"][sl].copy_(p64.reshape(n, 3), non_blocking=True)
+                t["pos"][sl].copy_(t["pos64"][sl], non_blocking=True)
+                bx64, b2 = self._src64(r.box)
+                t["box64"][a.slot].copy_(bx64.reshape(3, 3), non_blocking=True)
+                t["box"][a.slot].copy_(t["box64"][a.slot], non_blocking=True)
+            else:
+                pos, nb = self._src(r.pos, npdt)
+                t["pos"][sl].copy_(pos.reshape(n, 3), non_blocking=True)
+                bx, b2 = self._src(r.box, npdt)
+                t["box"][a.slot].copy_(bx.reshape(3, 3), non_blocking=True)
             nb += b2
             if a.kind == SYS_PME:
                 q, b3 = self._src(r.charges, npdt)

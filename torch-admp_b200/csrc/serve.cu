@@ -150,15 +150,18 @@ static int serve_neighbors_impl(const admp_pools* P, const admp_sys* sys, int ns
   const Batch& b = plan.b;
   typedef typename Vec4<T>::type V4;
   srv_table_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(c.L, P->box, sizeof(T) == 8, nullptr, ss, 1);
-  sn_setup_kernel<T><<<nsys, 256, 0, st>>>(b, ss, (const T*)P->box, P->cells);
-  sn_bin_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const T*)P->pos, (V4*)P->frac, P->cell_of, P->cells);
+  if (P->pos64 && !P->frac64) return fail(ADMP_ERR_BAD_ARG, "serve: pos64 needs a frac64 scratch");
+  const double4* f64 = P->pos64 ? (const double4*)P->frac64 : nullptr;
+  sn_setup_kernel<T><<<nsys, 256, 0, st>>>(b, ss, (const T*)P->box, P->box64, P->cells);
+  sn_bin_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const T*)P->pos, P->pos64, (V4*)P->frac,
+                                                P->pos64 ? (double4*)P->frac64 : nullptr, P->cell_of, P->cells);
   sn_scan_cells_kernel<<<nsys, 1024, 0, st>>>(ss, P->cells);
   sn_scatter_kernel<<<b.nblk_atom, 256, 0, st>>>(b, ss, P->cell_of, P->cells, P->sorted);
-  sn_pairs_kernel<T, false><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, P->cell_of, P->cells, P->sorted,
-                                                         P->pcnt, nullptr, nullptr);
+  sn_pairs_kernel<T, false><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, f64, P->cell_of, P->cells,
+                                                         P->sorted, P->pcnt, nullptr, nullptr);
   sn_scan_rows_kernel<<<nsys, 1024, 0, st>>>(b, ss, P->pcnt, P->pstart, P->slot_info);
-  sn_pairs_kernel<T, true><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, P->cell_of, P->cells, P->sorted,
-                                                        P->pcnt, P->pstart, P->col);
+  sn_pairs_kernel<T, true><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, f64, P->cell_of, P->cells,
+                                                        P->sorted, P->pcnt, P->pstart, P->col);
   count_launches(8);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;

@@ -50,12 +50,16 @@ __device__ __forceinline__ double4 make_v4<double>(double a, double b, double c,
 
 // one block per system: geometry, grid, zero the cell counters
 template <typename T>
-__global__ void sn_setup_kernel(Batch b, SrvSys* __restrict__ ss, const T* __restrict__ box, int* __restrict__ cells) {
+__global__ void sn_setup_kernel(Batch b, SrvSys* __restrict__ ss, const T* __restrict__ box,
+                                const double* __restrict__ box64, int* __restrict__ cells) {
   const int s = blockIdx.x;
   SrvSys& S = ss[s];
   __shared__ int nc_sh[4];
   if (threadIdx.x == 0) {
-    load_box(box + (size_t)b.s[s].box_idx * 9, S.b);
+    if (box64)
+      load_box(box64 + (size_t)b.s[s].box_idx * 9, S.b);
+    else
+      load_box(box + (size_t)b.s[s].box_idx * 9, S.b);
     const double V = inv3(S.b, S.bi);
     double h[3];
     for (int d = 0; d < 3; ++d) {
@@ -90,8 +94,9 @@ __global__ void sn_setup_kernel(Batch b, SrvSys* __restrict__ ss, const T* __res
 
 template <typename T>
 static __global__ void __launch_bounds__(256)
-    sn_bin_kernel(Batch b, SrvSys* __restrict__ ss, const T* __restrict__ pos, typename Vec4<T>::type* __restrict__ frac,
-                  int* __restrict__ cell_of, int* __restrict__ cells) {
+    sn_bin_kernel(Batch b, SrvSys* __restrict__ ss, const T* __restrict__ pos, const double* __restrict__ pos64,
+                  typename Vec4<T>::type* __restrict__ frac, double4* __restrict__ frac64, int* __restrict__ cell_of,
+                  int* __restrict__ cells) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc& d = b.s[s];
   const SrvSys& S = ss[s];
@@ -103,7 +108,9 @@ static __global__ void __launch_bounds__(256)
       cell_of[i] = -1;
       continue;
     }
-    const double r0 = pos[3 * (size_t)i], r1 = pos[3 * (size_t)i + 1], r2 = pos[3 * (size_t)i + 2];
+    const double r0 = pos64 ? pos64[3 * (size_t)i] : (double)pos[3 * (size_t)i];
+    const double r1 = pos64 ? pos64[3 * (size_t)i + 1] : (double)pos[3 * (size_t)i + 1];
+    const double r2 = pos64 ? pos64[3 * (size_t)i + 2] : (double)pos[3 * (size_t)i + 2];
     double f[3];
     int c[3];
     bool ok = isfinite(r0) && isfinite(r1) && isfinite(r2);
@@ -113,6 +120,7 @@ static __global__ void __launch_bounds__(256)
       c[e] = ok ? min((int)(f[e] * S.nc[e]), S.nc[e] - 1) : 0;
     }
     frac[i] = make_v4<T>((T)f[0], (T)f[1], (T)f[2], T(0));
+    if (frac64) frac64[i] = make_double4(f[0], f[1], f[2], 0.0);
     if (!ok) {
       cell_of[i] = -1;
       continue;
@@ -186,8 +194,9 @@ __device__ __forceinline__ void sn_offsets(int nc, int* off, int& n) {
 template <typename T, bool FILL>
 static __global__ void __launch_bounds__(256)
     sn_pairs_kernel(Batch b, const SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
-                    const int* __restrict__ cell_of, const int* __restrict__ cells, const int* __restrict__ sorted,
-                    int* __restrict__ pcnt, const long long* __restrict__ pstart, int* __restrict__ col) {
+                    const double4* __restrict__ frac64, const int* __restrict__ cell_of, const int* __restrict__ cells,
+                    const int* __restrict__ sorted, int* __restrict__ pcnt, const long long* __restrict__ pstart,
+                    int* __restrict__ col) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc& d = b.s[s];
   const SrvSys& S = ss[s];
@@ -210,7 +219,8 @@ static __global__ void __launch_bounds__(256)
     sn_offsets(nc0, o0, n0);
     sn_offsets(nc1, o1, n1);
     sn_offsets(nc2, o2, n2);
-    const typename Vec4<T>::type fi = frac[i];
+    const typename Vec4<T>::type fit = frac[i];
+    const double4 fi = frac64 ? frac64[i] : make_double4(fit.x, fit.y, fit.z, 0.0);
     int cnt = 0;
     const long long base = FILL ? pstart[i] : 0;
     for (int ia = 0; ia < n0; ++ia) {
@@ -223,8 +233,14 @@ static __global__ void __launch_bounds__(256)
           for (int t = start[cc]; t < start[cc + 1]; ++t) {
             const int j = sorted[d.atom_off + t];
             if (j == i) continue;
-            const typename Vec4<T>::type fj = frac[j];
-            double df[3] = {(double)fj.x - (double)fi.x, (double)fj.y - (double)fi.y, (double)fj.z - (double)fi.z};
+            double4 fj;
+            if (frac64) {
+              fj = frac64[j];
+            } else {
+              const typename Vec4<T>::type t = frac[j];
+              fj = make_double4(t.x, t.y, t.z, 0.0);
+            }
+            double df[3] = {fj.x - fi.x, fj.y - fi.y, fj.z - fi.z};
             for (int e = 0; e < 3; ++e) df[e] -= floor(df[e] + 0.5);
             double r2 = 0.0;
             for (int e = 0; e < 3; ++e) {

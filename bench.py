@@ -4,7 +4,7 @@ Workload (one "step" = one pass over the stream): N_REQ requests with atom
 counts log-uniform in [200, 20000], cubic boxes at 0.1 atoms/A^3, 60% PME
 energy+forces (+-1 charges) and 40% QEq solves on water-like systems, rc 6 A,
 ethresh 5e-4 (mesh from the reference's automatic rule), CG to
-||P grad|| / N < 1e-6.  Synthetic, seeded (the reference has no dataset).
+||P grad|| / N < 1e-7.  Synthetic, seeded (the reference has no dataset).
 
   value        systems/s of the batched FP32 serving engine with every input
                already resident in HBM (closed loop: all requests available)
@@ -43,7 +43,12 @@ UNIT = "systems/s"
 N_REQ = 2000
 SEED = 1024
 RATE = 2000.0          # Poisson arrival rate (requests/s) of the synthetic stream
-RCUT, ETHRESH, TOL = 6.0, 5e-4, 1e-6
+RCUT, ETHRESH = 6.0, 5e-4
+# CG stopping rule ||P grad||_2 / N < TOL; 1e-7 keeps the FP32 charges within 1e-5 e and the
+# forces within 1e-4 of the FP64 solution (at 1e-6 the charge error reaches ~5e-6 e and the
+# force error ~2e-4)
+TOL = 1e-7
+LAT_RATE = 1000.0      # open-loop Poisson rate (requests/s) for the p50/p99 latency pass
 
 
 def parse():
@@ -53,10 +58,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nreq", type=int, default=N_REQ)
-    ap.add_argument("--latency-rate", type=float, default=None,
-                    help="open-loop arrival rate for p50/p99 (default: 0.7 x measured e2e capacity)")
+    ap.add_argument("--latency-rate", type=float, default=LAT_RATE,
+                    help="open-loop Poisson arrival rate (requests/s) for p50/p99")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--plain-sample", type=int, default=24)
+    ap.add_argument("--plain-sample", type=int, default=100)
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -201,7 +206,7 @@ def to_device_requests(stream, dev, dtype):
     return out
 
 
-def plain_path(stream, dev, dtype, n):
+def plain_path(stream, dev, dtype, n, eps=TOL):
     """One system at a time through the drop-in modules (what a user of the
     reference API would run on the GPU)."""
     import torch
@@ -210,7 +215,7 @@ def plain_path(stream, dev, dtype, n):
     from admp_b200.pme import CoulombForceModule
     from admp_b200.qeq import QEqForceModule, pgrad_optimize
     cm = CoulombForceModule(rcut=RCUT, ethresh=ETHRESH)
-    qm = QEqForceModule(RCUT, ETHRESH, eps=TOL, max_iter=300)
+    qm = QEqForceModule(RCUT, ETHRESH, eps=eps, max_iter=2000)
     nb = TorchNeighborList(RCUT)
     out = {}
 
@@ -350,7 +355,7 @@ def main():
         e2e_val = args.nreq * world / float(t.item())
 
     # open-loop latency at a stated Poisson rate
-    lat_rate = args.latency_rate or 0.7 * (args.nreq / e2e_s)
+    lat_rate = args.latency_rate
     lat_res = one_pass(stream, to_host=True, arrivals=True, rate_scale=RATE / lat_rate)
     lats = sorted(r.latency for r in lat_res)
     p50 = lats[len(lats) // 2] * 1000.0
@@ -358,14 +363,19 @@ def main():
 
     # plain one-at-a-time GPU path and accuracy of the FP32 serving results vs FP64
     plain_val, plain_out = plain_path(stream, dev, torch.float32, args.plain_sample)
-    _, ref64 = plain_path(stream, dev, torch.float64, args.plain_sample)
+    # accuracy reference: FP64 drop-in path with the charge solve converged tightly (pinned to the oracle)
+    _, ref64 = plain_path(stream, dev, torch.float64, args.plain_sample, eps=1e-10)
     byrid = {r.rid: r for r in one_pass(stream, to_host=True)}
-    ferr, qerr = 0.0, 0.0
+    ferr, qerr, ferr_pme, ferr_qeq = 0.0, 0.0, 0.0, 0.0
     for rid, (E, F, q) in ref64.items():
         o = byrid[rid]
-        ferr = max(ferr, float(np.abs(o.forces - F).max() / np.abs(F).max()))
+        fe = float(np.abs(o.forces - F).max() / np.abs(F).max())
+        ferr = max(ferr, fe)
         if q is not None:
+            ferr_qeq = max(ferr_qeq, fe)
             qerr = max(qerr, float(np.abs(o.charges - q).max()))
+        else:
+            ferr_pme = max(ferr_pme, fe)
 
     # roofline of the dominant kernel
     import json as _json
@@ -405,7 +415,9 @@ def main():
                                                                      "one system per call"},
             "speedup_vs_plain": value / plain_val if plain_val else None,
             "accuracy": {"max_rel_force_err_vs_fp64": ferr, "max_charge_err_vs_fp64_e": qerr,
-                         "sample": f"first {args.plain_sample} requests vs the FP64 drop-in path"},
+                         "max_rel_force_err_pme": ferr_pme, "max_rel_force_err_qeq": ferr_qeq,
+                         "sample": f"first {args.plain_sample} requests vs the FP64 drop-in path "
+                                   "(QEq solved to ||P grad||/N < 1e-10)"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
                          "kernels": rf},

@@ -224,6 +224,8 @@ typedef struct admp_sys {
   int pad;
   long long pair_off;  /* first entry in the pair pools */
   long long pair_cap;  /* entries reserved for this system's neighbour rows */
+  long long green_off; /* QEq: first element of its cached Green's function in pools->green
+                        * (K0*K1*(K2/2+1) elements); unused for PME systems */
   double kappa;
   double rcut;
 } admp_sys;
@@ -264,6 +266,7 @@ typedef struct admp_pools {
   double* acc;         int acc_cap;          /* systems (32 doubles each) */
   int* cells;          long long cells_cap;  /* ints */
   void* sys_scratch;   long long sys_scratch_bytes;
+  void* green;         long long green_cap;  /* dtype: cached Green's functions of QEq slots */
   /* optional double copies used only for the neighbour decisions of FP32
    * pools (which pairs lie inside rc), so the pair set equals the FP64 one */
   double* pos64;       /* [A,3] or NULL */

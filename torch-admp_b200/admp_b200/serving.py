@@ -41,8 +41,8 @@ MAX_PER_LAUNCH = 128
 class AdmpSys(ctypes.Structure):
     _fields_ = [("natoms", ctypes.c_int), ("atom_off", ctypes.c_int), ("slot", ctypes.c_int),
                 ("kind", ctypes.c_int), ("kmesh", ctypes.c_int * 3), ("pad", ctypes.c_int),
-                ("pair_off", ctypes.c_longlong), ("pair_cap", ctypes.c_longlong), ("kappa", ctypes.c_double),
-                ("rcut", ctypes.c_double)]
+                ("pair_off", ctypes.c_longlong), ("pair_cap", ctypes.c_longlong), ("green_off", ctypes.c_longlong),
+                ("kappa", ctypes.c_double), ("rcut", ctypes.c_double)]
 
 
 _P = ctypes.c_void_p
@@ -54,7 +54,8 @@ class AdmpPools(ctypes.Structure):
                                   "cg_diag", "cg_z", "cg_chi", "cg_hx", "cg_p", "cg_hp", "mesh")] + \
                [("mesh_cap", ctypes.c_longlong), ("spec", _P), ("spec_cap", ctypes.c_longlong), ("acc", _P),
                 ("acc_cap", ctypes.c_int), ("cells", _P), ("cells_cap", ctypes.c_longlong), ("sys_scratch", _P),
-                ("sys_scratch_bytes", ctypes.c_longlong), ("pos64", _P), ("box64", _P), ("frac64", _P)]
+                ("sys_scratch_bytes", ctypes.c_longlong), ("green", _P), ("green_cap", ctypes.c_longlong),
+                ("pos64", _P), ("box64", _P), ("frac64", _P)]
 
 
 def _bind_serve(lib):
@@ -140,6 +141,8 @@ class _Active:
     kmesh: List[int]
     kind: int
     t_arrival: float
+    green_off: int = -1
+    green_n: int = 0
     retries: int = 0
 
 
@@ -152,7 +155,7 @@ class ServingEngine:
     def __init__(self, device="cuda:0", dtype=torch.float32, max_atoms: int = 4_000_000, max_slots: int = 512,
                  pairs_per_atom: float = 150.0, mesh_budget: int = 64_000_000, rcut: float = 6.0,
                  ethresh: float = 5e-4, tol: float = 1e-6, max_iter: int = 300, iters_per_tick: int = 8,
-                 ke: float = DIELECTRIC):
+                 ke: float = DIELECTRIC, green_budget: Optional[int] = None):
         self.lib = L.load()
         _bind_serve(self.lib)
         self.dev = torch.device(device)
@@ -185,6 +188,7 @@ class ServingEngine:
             "cells": torch.zeros(3 * (2 * A + 129 * MAX_PER_LAUNCH), **i32),
             "sys_scratch": torch.zeros(self.lib.admp_serve_sys_scratch_bytes(MAX_PER_LAUNCH), dtype=torch.uint8,
                                        device=self.dev),
+            "green": torch.zeros(green_budget if green_budget is not None else mesh_budget, **f),
         }
         if dtype == torch.float32:
             # double copies for the neighbour decisions: the FP32 pair set equals the FP64 one
@@ -195,7 +199,7 @@ class ServingEngine:
         self.pools = AdmpPools()
         for name in ("pos", "q", "chi", "hardness", "eta", "force", "frac", "pstart", "pcnt", "cell_of", "sorted",
                      "col", "coef", "box", "energy", "cg_state", "slot_info", "cg_x", "cg_r", "cg_diag", "cg_z",
-                     "cg_chi", "cg_hx", "cg_p", "cg_hp", "mesh", "spec", "acc", "cells", "sys_scratch"):
+                     "cg_chi", "cg_hx", "cg_p", "cg_hp", "mesh", "spec", "acc", "cells", "sys_scratch", "green"):
             setattr(self.pools, name, t[name].data_ptr())
         for name in ("pos64", "box64", "frac64"):
             setattr(self.pools, name, t[name].data_ptr() if name in t else None)
@@ -204,6 +208,8 @@ class ServingEngine:
         self.pools.acc_cap = MAX_PER_LAUNCH
         self.pools.cells_cap = t["cells"].numel()
         self.pools.sys_scratch_bytes = t["sys_scratch"].numel()
+        self.pools.green_cap = t["green"].numel()
+        self.greens = _Intervals(t["green"].numel(), 32)
         self.mesh_budget = mesh_budget
         self.atoms = _Intervals(A, 32)
         self.pairs = _Intervals(Pn, 64)
@@ -258,6 +264,7 @@ class ServingEngine:
                 s.kmesh[d] = a.kmesh[d]
             s.pair_off = a.pair_off
             s.pair_cap = a.pair_cap
+            s.green_off = a.green_off
             s.kappa = self.kappa
             s.rcut = self.rcut
         return arr
@@ -284,11 +291,18 @@ class ServingEngine:
             L.check(st, fn.__name__)
 
     def _admit(self, now: float) -> List[_Active]:
-        admitted = []
-        mesh_in_tick = 0
-        keep = []
+        """Admit arrived requests while slots and pool space allow.  Within a
+        tick PME requests are placed before QEq requests, so that each kind
+        occupies one contiguous run of the atom pool and uploads in one copy
+        per field."""
+        ready, keep = [], []
         for req, tarr in self.queue:
-            if tarr > now:
+            (ready if tarr <= now else keep).append((req, tarr))
+        ready.sort(key=lambda rt: 0 if rt[0].kind == "pme" else 1)
+        admitted = []
+        blocked = False
+        for req, tarr in ready:
+            if blocked:
                 keep.append((req, tarr))
                 continue
             n = req.natoms
@@ -307,116 +321,161 @@ class ServingEngine:
                 self.atoms.release(aoff, n)
                 keep.append((req, tarr))
                 continue
+            kind = SYS_QEQ if req.kind == "qeq" else SYS_PME
+            goff, gn = -1, 0
+            if kind == SYS_QEQ:
+                gn = km[0] * km[1] * (km[2] // 2 + 1)
+                goff = self.greens.alloc(gn)
+                if goff is None:
+                    self.atoms.release(aoff, n)
+                    self.pairs.release(poff, pcap)
+                    keep.append((req, tarr))
+                    continue
             slot = self.free_slots.pop()
-            a = _Active(req, slot, aoff, poff, pcap, km, SYS_QEQ if req.kind == "qeq" else SYS_PME, tarr)
-            admitted.append(a)
-            mesh_in_tick += m
+            admitted.append(_Active(req, slot, aoff, poff, pcap, km, kind, tarr, goff, gn))
+        keep.sort(key=lambda rt: rt[1])
         self.queue = keep
         if admitted:
             self._upload(admitted)
             self.stats["admitted"] += len(admitted)
         return admitted
 
-    def _src(self, x, npdt):
-        """Source tensor for a request array: device tensors are used as they
-        are (device-to-device copy), host arrays go through pinned memory."""
-        if isinstance(x, torch.Tensor):
-            return x.to(self.dtype), 0
-        t = torch.from_numpy(np.ascontiguousarray(x, dtype=npdt)).pin_memory()
-        return t, t.numel() * t.element_size()
+    @staticmethod
+    def _runs(items: List[_Active]):
+        """Maximal runs of items whose atom regions are back to back."""
+        runs, cur = [], []
+        for a in items:
+            if cur and cur[-1].atom_off + cur[-1].req.natoms != a.atom_off:
+                runs.append(cur)
+                cur = []
+            cur.append(a)
+        if cur:
+            runs.append(cur)
+        return runs
 
-    def _src64(self, x):
-        if isinstance(x, torch.Tensor):
-            return x.to(torch.float64), 0
-        t = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).pin_memory()
+    def _stack(self, arrays, dtype):
+        """Concatenate request arrays into one source tensor: device tensors
+        with torch.cat, host arrays through one pinned buffer.  Returns
+        (tensor, host bytes)."""
+        if isinstance(arrays[0], torch.Tensor):
+            return torch.cat([a.reshape(-1).to(dtype) for a in arrays]), 0
+        npdt = {torch.float32: np.float32, torch.float64: np.float64}[dtype]
+        host = np.concatenate([np.asarray(a, dtype=npdt).reshape(-1) for a in arrays])
+        t = torch.from_numpy(host).pin_memory()
         return t, t.numel() * t.element_size()
 
     def _upload(self, items: List[_Active]) -> None:
         t = self.t
-        npdt = np.float32 if self.dtype == torch.float32 else np.float64
-        for a in items:
-            r = a.req
-            n = r.natoms
-            sl = slice(a.atom_off, a.atom_off + n)
-            if "pos64" in t:
-                # positions and box arrive in double; the FP32 copies are made on the device
-                p64, nb = self._src64(r.pos)
-                t["pos64"][sl].copy_(p64.reshape(n, 3), non_blocking=True)
+        nb = 0
+        has64 = "pos64" in t
+        slots = torch.tensor([a.slot for a in items], dtype=torch.long).to(self.dev, non_blocking=True)
+        boxes, b = self._stack([a.req.box for a in items], torch.float64 if has64 else self.dtype)
+        nb += b
+        boxes = boxes.to(self.dev, non_blocking=True).reshape(-1, 3, 3)
+        if has64:
+            t["box64"].index_copy_(0, slots, boxes)
+        t["box"].index_copy_(0, slots, boxes.to(self.dtype))
+        for run in self._runs(items):
+            lo = run[0].atom_off
+            hi = run[-1].atom_off + run[-1].req.natoms
+            sl = slice(lo, hi)
+            pos, b = self._stack([a.req.pos for a in run], torch.float64 if has64 else self.dtype)
+            nb += b
+            if has64:
+                # positions arrive in double; the FP32 copy is made on the device
+                t["pos64"][sl].copy_(pos.reshape(-1, 3), non_blocking=True)
                 t["pos"][sl].copy_(t["pos64"][sl], non_blocking=True)
-                bx64, b2 = self._src64(r.box)
-                t["box64"][a.slot].copy_(bx64.reshape(3, 3), non_blocking=True)
-                t["box"][a.slot].copy_(t["box64"][a.slot], non_blocking=True)
             else:
-                pos, nb = self._src(r.pos, npdt)
-                t["pos"][sl].copy_(pos.reshape(n, 3), non_blocking=True)
-                bx, b2 = self._src(r.box, npdt)
-                t["box"][a.slot].copy_(bx.reshape(3, 3), non_blocking=True)
-            nb += b2
-            if a.kind == SYS_PME:
-                q, b3 = self._src(r.charges, npdt)
-                t["q"][sl].copy_(q, non_blocking=True)
-                nb += b3
-            else:
-                for name, arr in (("chi", r.chi), ("hardness", r.hardness), ("eta", r.eta)):
-                    v, b3 = self._src(arr, npdt)
-                    t[name][sl].copy_(v, non_blocking=True)
-                    nb += b3
-                key = r.meta.get("system_id") if r.meta else None
-                w = self.warm.get(key) if key is not None else None
-                if w is not None and len(w) == n:
-                    t["q"][sl].copy_(w.to(self.dtype) if isinstance(w, torch.Tensor)
-                                     else torch.from_numpy(np.asarray(w, dtype=npdt)), non_blocking=True)
+                t["pos"][sl].copy_(pos.reshape(-1, 3), non_blocking=True)
+            # runs of one kind (PME first, then QEq, within a tick)
+            k = 0
+            while k < len(run):
+                j = k
+                while j < len(run) and run[j].kind == run[k].kind:
+                    j += 1
+                sub = run[k:j]
+                ssl = slice(sub[0].atom_off, sub[-1].atom_off + sub[-1].req.natoms)
+                if sub[0].kind == SYS_PME:
+                    q, b = self._stack([a.req.charges for a in sub], self.dtype)
+                    t["q"][ssl].copy_(q, non_blocking=True)
+                    nb += b
                 else:
-                    t["q"][sl].zero_()
-            self.stats["h2d_bytes"] += nb
+                    for name in ("chi", "hardness", "eta"):
+                        v, b = self._stack([getattr(a.req, name) for a in sub], self.dtype)
+                        t[name][ssl].copy_(v, non_blocking=True)
+                        nb += b
+                    t["q"][ssl].zero_()
+                    for a in sub:
+                        key = a.req.meta.get("system_id") if a.req.meta else None
+                        w = self.warm.get(key) if key is not None else None
+                        if w is not None and len(w) == a.req.natoms:
+                            src = w.to(self.dtype) if isinstance(w, torch.Tensor) else torch.from_numpy(
+                                np.asarray(w, dtype=np.float32 if self.dtype == torch.float32 else np.float64))
+                            t["q"][a.atom_off:a.atom_off + a.req.natoms].copy_(src, non_blocking=True)
+                k = j
+        self.stats["h2d_bytes"] += nb
 
     def _finish(self, items: List[_Active], now_fn) -> None:
-        """Energy + forces of finished systems, results out, resources freed."""
+        """Energy + forces of finished systems, results out, resources freed.
+        Forces (and QEq charges) of all finished systems leave the device in
+        one gather + one copy."""
         if not items:
             return
         self._call(self.lib.admp_serve_energy_forces, items, self.ke)
         t = self.t
         host = self.results_to_host
-        outs = []
-        for a in items:
-            n = a.req.natoms
-            sl = slice(a.atom_off, a.atom_off + n)
-            q = None
-            if host:
-                F = torch.empty((n, 3), dtype=self.dtype, pin_memory=True)
-                F.copy_(t["force"][sl], non_blocking=True)
-                if a.kind == SYS_QEQ:
-                    q = torch.empty(n, dtype=self.dtype, pin_memory=True)
-                    q.copy_(t["q"][sl], non_blocking=True)
-            else:
-                F = t["force"][sl].clone()
-                if a.kind == SYS_QEQ:
-                    q = t["q"][sl].clone()
-            outs.append((a, F, q))
+        runs = self._runs(sorted(items, key=lambda a: a.atom_off))
+        F_all = torch.cat([t["force"][r[0].atom_off:r[-1].atom_off + r[-1].req.natoms] for r in runs])
+        qitems = [a for a in items if a.kind == SYS_QEQ]
+        qruns = self._runs(sorted(qitems, key=lambda a: a.atom_off))
+        q_all = torch.cat([t["q"][r[0].atom_off:r[-1].atom_off + r[-1].req.natoms] for r in qruns]) if qruns else None
+        if host:
+            Fh = torch.empty(F_all.shape, dtype=self.dtype, pin_memory=True)
+            Fh.copy_(F_all, non_blocking=True)
+            qh = None
+            if q_all is not None:
+                qh = torch.empty(q_all.shape, dtype=self.dtype, pin_memory=True)
+                qh.copy_(q_all, non_blocking=True)
+            F_all, q_all = Fh, qh
         E = torch.empty(self.max_slots, dtype=torch.float64, pin_memory=True)
         E.copy_(t["energy"], non_blocking=True)
         info = torch.empty(self.max_slots, 4, dtype=torch.int32, pin_memory=True)
         info.copy_(t["slot_info"], non_blocking=True)
         self.stream.synchronize()
         tdone = now_fn()
-        for a, F, q in outs:
-            st = int(info[a.slot, 2])
-            it = int(info[a.slot, 1]) if a.kind == SYS_QEQ else 0
+        Fsrc = F_all.numpy() if host else F_all
+        qsrc = (q_all.numpy() if host else q_all) if q_all is not None else None
+        Eh = E.numpy()
+        ih = info.numpy()
+        off, qoff = {}, {}
+        o = 0
+        for r in runs:
+            for a in r:
+                off[a.slot] = o
+                o += a.req.natoms
+        o = 0
+        for r in qruns:
+            for a in r:
+                qoff[a.slot] = o
+                o += a.req.natoms
+        for a in items:
+            n = a.req.natoms
+            Fo = Fsrc[off[a.slot]:off[a.slot] + n]
+            qo = qsrc[qoff[a.slot]:qoff[a.slot] + n] if a.kind == SYS_QEQ else None
+            st = int(ih[a.slot, 2])
+            it = int(ih[a.slot, 1]) if a.kind == SYS_QEQ else 0
             if host:
-                Fo = F.numpy().copy()
-                qo = q.numpy().copy() if q is not None else None
-                self.stats["d2h_bytes"] += F.numel() * F.element_size() + 8 + (
-                    q.numel() * q.element_size() if q is not None else 0)
-            else:
-                Fo, qo = F, q
+                self.stats["d2h_bytes"] += n * 3 * Fsrc.itemsize + 8 + (n * qsrc.itemsize if qo is not None else 0)
             if qo is not None and a.req.meta and a.req.meta.get("system_id") is not None:
-                self.warm[a.req.meta["system_id"]] = qo.copy() if host else qo
-            self.results.append(Result(a.req.rid, a.req.kind, float(E[a.slot]), Fo, qo, it, st, a.t_arrival, tdone))
+                self.warm[a.req.meta["system_id"]] = qo.copy() if host else qo.clone()
+            self.results.append(Result(a.req.rid, a.req.kind, float(Eh[a.slot]), Fo, qo, it, st, a.t_arrival, tdone))
             self._release(a)
 
     def _release(self, a: _Active) -> None:
         self.atoms.release(a.atom_off, a.req.natoms)
         self.pairs.release(a.pair_off, a.pair_cap)
+        if a.green_off >= 0:
+            self.greens.release(a.green_off, a.green_n)
         self.free_slots.append(a.slot)
 
     def tick(self, now_fn=time.perf_counter) -> int:

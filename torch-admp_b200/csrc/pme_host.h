@@ -14,6 +14,7 @@ struct SysSpec {
   int K[3];
   double kappa;
   int box_idx;
+  long long green_off = -1;  // cached Green's function offset; -1: same as the spectrum offset
 };
 
 // Launch geometry of a batch.
@@ -23,6 +24,12 @@ struct RecipPlan {
   size_t mesh_elems = 0;  // real mesh elements (all systems)
   size_t spec_elems = 0;  // complex spectrum elements
   size_t smem_z = 0, smem_y = 0, smem_x = 0;
+  // fused slab passes: one block per x plane (blk_slab offsets), when a plane fits
+  bool slab = false;
+  int buf_elems = 0;
+  size_t smem_slab = 0;
+  int nblk_slab = 0;
+  int blk_slab[kMaxBatch];
 };
 
 template <typename T>
@@ -30,7 +37,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   if (nsys <= 0 || nsys > kMaxBatch) return fail(ADMP_ERR_BAD_ARG, "batch of %d systems (max %d)", nsys, kMaxBatch);
   Batch& b = p.b;
   b.nsys = nsys;
-  b.apb = 32;
+  b.apb = 256;
   b.done = nullptr;
   b.done_stride = 0;
   int maxK[3] = {1, 1, 1};
@@ -78,6 +85,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
     d.blk_x = bx;
     d.mesh_off = (int64_t)mo;
     d.spec_off = (int64_t)so;
+    d.green_off = sys[s].green_off >= 0 ? (int64_t)sys[s].green_off : (int64_t)so;
     const int ncb = (d.K2h + zb - 1) / zb;
     ba += (d.natoms + b.apb - 1) / b.apb;
     bz += ((d.K0 * d.K1 + 1) / 2 + lp - 1) / lp;
@@ -92,44 +100,103 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   b.nblk_x = bx;
   p.mesh_elems = mo;
   p.spec_elems = so;
+  // fused slab passes: buffers of max(ceil(K1/2) K2, K1 (K2/2+1)) complex, two of them, plus twiddles
+  int be = 0;
+  for (int s = 0; s < nsys; ++s) {
+    const int a = ((sys[s].K[1] + 1) / 2) * sys[s].K[2];
+    const int c = sys[s].K[1] * (sys[s].K[2] / 2 + 1);
+    be = be > a ? be : a;
+    be = be > c ? be : c;
+  }
+  p.buf_elems = be;
+  p.smem_slab = (2 * (size_t)be + maxK[1] + maxK[2]) * cs;
+  p.slab = p.smem_slab <= 200 * 1024;
+  p.nblk_slab = 0;
+  for (int s = 0; s < nsys; ++s) {
+    p.blk_slab[s] = p.nblk_slab;
+    p.nblk_slab += sys[s].K[0];
+  }
   return ADMP_OK;
 }
 
 // Mesh -> potential: the five FFT passes with the Green's function.
+// 2 G_s for every half-spectrum point of the batch, at each system's green_off
+template <typename T>
+inline int launch_green_build(const RecipPlan<T>& p, const T* box, T* green, double ke, cudaStream_t st) {
+  if (p.b.nblk_x) green_build_kernel<T><<<p.b.nblk_x, 256, 0, st>>>(p.b, box, green, ke);
+  count_launches(1);
+  ADMP_CUDA_TRY(cudaGetLastError());
+  return ADMP_OK;
+}
+
 template <typename T>
 inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const T* box, double* acc, double ke,
-                            cudaStream_t st) {
+                            cudaStream_t st, const T* green = nullptr) {
   const Batch& b = p.b;
   ADMP_CUDA_TRY(ensure_smem(fft_z_fwd_kernel<T>, p.smem_z));
   ADMP_CUDA_TRY(ensure_smem(fft_z_inv_kernel<T>, p.smem_z));
   ADMP_CUDA_TRY(ensure_smem(fft_y_kernel<T, false>, p.smem_y));
   ADMP_CUDA_TRY(ensure_smem(fft_y_kernel<T, true>, p.smem_y));
   ADMP_CUDA_TRY(ensure_smem(fft_x_green_kernel<T>, p.smem_x));
+  ADMP_CUDA_TRY(ensure_smem(fft_x_apply_kernel<T>, p.smem_x));
   // algorithmic bytes: z passes read/write M reals + Mh complex, y/x passes Mh complex in and out
   const double rb = (double)p.mesh_elems * sizeof(T), cb = (double)p.spec_elems * sizeof(Cplx<T>);
   int h;
+  Batch bs;  // slab launches: F_Y block offsets remapped to one block per x plane
+  if (p.slab) {
+    bs = b;
+    for (int s = 0; s < b.nsys; ++s) bs.s[s].blk_y = p.blk_slab[s];
+    bs.nblk_y = p.nblk_slab;
+    ADMP_CUDA_TRY(ensure_smem(fft_slab_fwd_kernel<T>, p.smem_slab));
+    ADMP_CUDA_TRY(ensure_smem(fft_slab_inv_kernel<T>, p.smem_slab));
+    h = prof_begin(st);
+    if (bs.nblk_y) fft_slab_fwd_kernel<T><<<bs.nblk_y, 256, p.smem_slab, st>>>(bs, mesh, spec, p.buf_elems);
+    prof_end(h, PK_FFT_Z_FWD, rb + cb, st);
+  } else {
+    h = prof_begin(st);
+    if (b.nblk_z) fft_z_fwd_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, mesh, spec);
+    prof_end(h, PK_FFT_Z_FWD, rb + cb, st);
+    h = prof_begin(st);
+    if (b.nblk_y) fft_y_kernel<T, false><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
+    prof_end(h, PK_FFT_Y_FWD, 2 * cb, st);
+  }
   h = prof_begin(st);
-  if (b.nblk_z) fft_z_fwd_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, mesh, spec);
-  prof_end(h, PK_FFT_Z_FWD, rb + cb, st);
-  h = prof_begin(st);
-  if (b.nblk_y) fft_y_kernel<T, false><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
-  prof_end(h, PK_FFT_Y_FWD, 2 * cb, st);
-  h = prof_begin(st);
-  if (b.nblk_x) fft_x_green_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(b, spec, box, acc, ke);
+  if (b.nblk_x) {
+    if (green)
+      fft_x_apply_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(b, spec, green);
+    else
+      fft_x_green_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(b, spec, box, acc, ke);
+  }
   prof_end(h, PK_FFT_X_GREEN, 2 * cb, st);
-  h = prof_begin(st);
-  if (b.nblk_y) fft_y_kernel<T, true><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
-  prof_end(h, PK_FFT_Y_INV, 2 * cb, st);
-  h = prof_begin(st);
-  if (b.nblk_z) fft_z_inv_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, spec, mesh);
-  prof_end(h, PK_FFT_Z_INV, rb + cb, st);
-  count_launches(5);
+  if (p.slab) {
+    h = prof_begin(st);
+    if (bs.nblk_y) fft_slab_inv_kernel<T><<<bs.nblk_y, 256, p.smem_slab, st>>>(bs, spec, mesh, p.buf_elems);
+    prof_end(h, PK_FFT_Z_INV, rb + cb, st);
+    count_launches(3);
+  } else {
+    h = prof_begin(st);
+    if (b.nblk_y) fft_y_kernel<T, true><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
+    prof_end(h, PK_FFT_Y_INV, 2 * cb, st);
+    h = prof_begin(st);
+    if (b.nblk_z) fft_z_inv_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, spec, mesh);
+    prof_end(h, PK_FFT_Z_INV, rb + cb, st);
+    count_launches(5);
+  }
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
 }
 
 // Full reciprocal evaluation: spread q, FFT/Green, gather.
 // `dE_dq` receives the potential (dE/dq), `dE_dpos` the gradient; both accumulate.
+template <typename T>
+inline size_t spread_smem() {
+  return 8 * WarpStencil<T, false>::bytes();
+}
+template <typename T, bool F>
+inline size_t gather_smem() {
+  return 8 * WarpStencil<T, F>::bytes();
+}
+
 template <typename T>
 inline double plan_atoms(const RecipPlan<T>& p) {
   double n = 0;
@@ -139,19 +206,23 @@ inline double plan_atoms(const RecipPlan<T>& p) {
 
 template <typename T>
 inline int launch_recip(const RecipPlan<T>& p, const T* pos, const T* box, const T* q, T* mesh, Cplx<T>* spec,
-                        double* acc, double ke, T* dE_dq, T* dE_dpos, cudaStream_t st) {
+                        double* acc, double ke, T* dE_dq, T* dE_dpos, cudaStream_t st,
+                        const int* order = nullptr) {
   const Batch& b = p.b;
   const double na = plan_atoms(p), mb = (double)p.mesh_elems * sizeof(T);
   ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
   int h = prof_begin(st);
-  if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, q, mesh);
+  ADMP_CUDA_TRY(ensure_smem(spread_kernel<T>, spread_smem<T>()));
+  ADMP_CUDA_TRY(ensure_smem(gather_kernel<T, true>, gather_smem<T, true>()));
+  if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, spread_smem<T>(), st>>>(b, pos, box, q, mesh, order);
   prof_end(h, PK_SPREAD, na * 4 * sizeof(T) + mb, st);
   count_launches(1);
   int s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st);
   if (s) return s;
   h = prof_begin(st);
   if (b.nblk_atom)
-    gather_kernel<T, true><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, q, mesh, dE_dq, dE_dpos, acc, T(1));
+    gather_kernel<T, true><<<b.nblk_atom, 256, gather_smem<T, true>(), st>>>(b, pos, box, q, mesh, dE_dq, dE_dpos,
+                                                                             acc, T(1), order);
   prof_end(h, PK_GATHER, mb + na * 4 * sizeof(T) + na * 3 * sizeof(T), st);
   count_launches(1);
   ADMP_CUDA_TRY(cudaGetLastError());
@@ -161,18 +232,22 @@ inline int launch_recip(const RecipPlan<T>& p, const T* pos, const T* box, const
 // Potential only (for the CG matvec): phi_i = dE/dq_i of the charges v.
 template <typename T>
 inline int launch_recip_potential(const RecipPlan<T>& p, const T* pos, const T* box, const T* v, T* mesh,
-                                  Cplx<T>* spec, double* acc, double ke, T* pot, cudaStream_t st) {
+                                  Cplx<T>* spec, double* acc, double ke, T* pot, cudaStream_t st,
+                                  const int* order = nullptr, const T* green = nullptr) {
   const Batch& b = p.b;
   const double na = plan_atoms(p), mb = (double)p.mesh_elems * sizeof(T);
   ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
   int h = prof_begin(st);
-  if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, v, mesh);
+  ADMP_CUDA_TRY(ensure_smem(spread_kernel<T>, spread_smem<T>()));
+  ADMP_CUDA_TRY(ensure_smem(gather_kernel<T, false>, gather_smem<T, false>()));
+  if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, spread_smem<T>(), st>>>(b, pos, box, v, mesh, order);
   prof_end(h, PK_SPREAD, na * 4 * sizeof(T) + mb, st);
-  int s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st);
+  int s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st, green);
   if (s) return s;
   h = prof_begin(st);
   if (b.nblk_atom)
-    gather_kernel<T, false><<<b.nblk_atom, 256, 0, st>>>(b, pos, box, v, mesh, pot, nullptr, acc, T(1));
+    gather_kernel<T, false><<<b.nblk_atom, 256, gather_smem<T, false>(), st>>>(b, pos, box, v, mesh, pot, nullptr,
+                                                                               acc, T(1), order);
   prof_end(h, PK_GATHER, mb + na * 4 * sizeof(T) + na * sizeof(T), st);
   count_launches(2);
   ADMP_CUDA_TRY(cudaGetLastError());

@@ -23,6 +23,7 @@ struct SysDesc {
   int32_t K0, K1, K2, K2h;
   int32_t blk_atom, blk_z, blk_y, blk_x;
   int64_t mesh_off, spec_off;
+  int64_t green_off;  // cached 2 G_s (half-spectrum layout) for CG matvecs
   double kappa;
   int32_t box_idx;
   int32_t flags;
@@ -126,12 +127,92 @@ __device__ __forceinline__ void make_stencil(const T* r, const Geom& g, int K0, 
 }
 
 // ---------------------------------------------------------------------------
-// spread: warp per atom, 216 atomic adds per atom into a zeroed mesh.
+// Warp-cooperative stencils: each lane builds the stencil of one atom (its
+// 3x6 B-spline weights, derivatives and wrapped mesh indices) into shared
+// memory, then the warp walks those 32 atoms with its lanes spread over the
+// 36 (y, z) stencil columns, each lane looping over the 6 x offsets.  The
+// optional `order` visits atoms in cell-sorted order so that neighbouring
+// atoms touch neighbouring mesh lines.
 // ---------------------------------------------------------------------------
+// Per-warp shared layout (dynamic shared memory): for 32 atoms, the 18
+// weights, optionally the 18 derivatives, x offsets ix*K1*K2 (6 ints), the
+// wrapped y / z stencil bases, the charge and the atom index.
+template <typename T, bool DERIV>
+struct WarpStencil {
+  T* w;     // [32][18]
+  T* dw;    // [32][18]
+  int* ox;  // [32][6]
+  int* byz; // [32][2]
+  T* q;     // [32]
+  int* atom;// [32]
+  __host__ __device__ static constexpr size_t bytes() {
+    return 32 * 18 * sizeof(T) * (DERIV ? 2 : 1) + 32 * 6 * sizeof(int) + 32 * 2 * sizeof(int) + 32 * sizeof(T) +
+           32 * sizeof(int) + 16;
+  }
+  __device__ void carve(unsigned char* base) {
+    w = reinterpret_cast<T*>(base);
+    T* e = w + 32 * 18;
+    if (DERIV) {
+      dw = e;
+      e += 32 * 18;
+    } else {
+      dw = nullptr;
+    }
+    q = e;
+    int* ip = reinterpret_cast<int*>(q + 32);
+    ox = ip;
+    byz = ox + 32 * 6;
+    atom = byz + 32 * 2;
+  }
+};
+
+template <typename T, bool DERIV>
+__device__ __forceinline__ void warp_build_stencil(WarpStencil<T, DERIV>& ws, const SysDesc& d, const Geom& g,
+                                                   const T* __restrict__ pos, const T* __restrict__ q,
+                                                   const int* __restrict__ order, int a_first, int a_end, int lane) {
+  const int a = a_first + lane;
+  if (a < a_end) {
+    const int ga = order ? order[d.atom_off + a] : d.atom_off + a;
+    T r[3] = {pos[3 * (size_t)ga], pos[3 * (size_t)ga + 1], pos[3 * (size_t)ga + 2]};
+    Stencil<T> st;
+    make_stencil<T>(r, g, d.K0, d.K1, d.K2, st);
+    T* w = ws.w + lane * 18;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      w[k] = st.w[0][k];
+      w[6 + k] = st.w[1][k];
+      w[12 + k] = st.w[2][k];
+      ws.ox[lane * 6 + k] = st.ix[k] * d.K1 * d.K2;
+    }
+    if (DERIV) {
+      T* dw = ws.dw + lane * 18;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        dw[k] = st.dw[0][k];
+        dw[6 + k] = st.dw[1][k];
+        dw[12 + k] = st.dw[2][k];
+      }
+    }
+    ws.byz[lane * 2] = st.iy[0];
+    ws.byz[lane * 2 + 1] = st.iz[0];
+    ws.q[lane] = q ? q[ga] : T(0);
+    ws.atom[lane] = ga;
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ int wrap_up(int i, int K) {
+  while (i >= K) i -= K;
+  return i;
+}
+
+// spread: q -> mesh (zeroed), atomic adds
 template <typename T>
 __global__ void __launch_bounds__(256) spread_kernel(Batch b, const T* __restrict__ pos,
                                                      const T* __restrict__ box,
-                                                     const T* __restrict__ q, T* __restrict__ mesh) {
+                                                     const T* __restrict__ q, T* __restrict__ mesh,
+                                                     const int* __restrict__ order) {
+  extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ Geom g;
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
@@ -139,21 +220,33 @@ __global__ void __launch_bounds__(256) spread_kernel(Batch b, const T* __restric
   load_geom(box, d.box_idx, &g);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
   const int a_begin = (blockIdx.x - d.blk_atom) * b.apb;
   const int a_end = min(a_begin + b.apb, d.natoms);
   T* M = mesh + d.mesh_off;
-  for (int a = a_begin + warp; a < a_end; a += blockDim.x >> 5) {
-    const int ga = d.atom_off + a;
-    const T qa = q[ga];
-    if (qa == T(0)) continue;
-    T r[3] = {pos[3 * (size_t)ga], pos[3 * (size_t)ga + 1], pos[3 * (size_t)ga + 2]};
-    Stencil<T> st;
-    make_stencil<T>(r, g, d.K0, d.K1, d.K2, st);
-    for (int p = lane; p < kStencil; p += 32) {
-      const int dx = p / 36, dy = (p / 6) % 6, dz = p % 6;
-      const size_t idx = ((size_t)st.ix[dx] * d.K1 + st.iy[dy]) * d.K2 + st.iz[dz];
-      atomicAdd(M + idx, qa * st.w[0][dx] * st.w[1][dy] * st.w[2][dz]);
+  WarpStencil<T, false> ws;
+  ws.carve(dsm + warp * WarpStencil<T, false>::bytes());
+  const int y0 = lane / 6, z0 = lane % 6, y1 = (lane + 32) / 6, z1 = (lane + 32) % 6;
+  for (int a0 = a_begin + warp * 32; a0 < a_end; a0 += nw * 32) {
+    warp_build_stencil<T, false>(ws, d, g, pos, q, order, a0, a_end, lane);
+    const int na = min(32, a_end - a0);
+    for (int j = 0; j < na; ++j) {
+      const T qa = ws.q[j];
+      if (qa == T(0)) continue;
+      const T* w = ws.w + j * 18;
+      const int* ox = ws.ox + j * 6;
+      const int by = ws.byz[2 * j], bz = ws.byz[2 * j + 1];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (h == 1 && lane >= 4) break;
+        const int yy = h ? y1 : y0, zz = h ? z1 : z0;
+        const T wyz = qa * w[6 + yy] * w[12 + zz];
+        const int oyz = wrap_up(by + yy, d.K1) * d.K2 + wrap_up(bz + zz, d.K2);
+#pragma unroll
+        for (int dx = 0; dx < 6; ++dx) atomicAdd(M + ox[dx] + oyz, w[dx] * wyz);
+      }
     }
+    __syncwarp();
   }
 }
 
@@ -295,8 +388,13 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
     Cplx<T> S = R[x * zb + c];
     const double s2 = (double)S.x * (double)S.x + (double)S.y * (double)S.y;
     double Gs = 0.0;
+    // the mirror label equals -n unless an x or y index is a Nyquist index; then
+    // G(mirror) = G(n) and one evaluation counts twice
+    const bool same = (n0b == -n0) && (nyb == -ny) && (n2b == -n2);
+    const double mult = same ? 2.0 : 1.0;
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
+      if (m == 1 && same) break;
       const int a0 = m ? n0b : n0, a1 = m ? nyb : ny, a2 = m ? n2b : n2;
       if (a0 == 0 && a1 == 0 && a2 == 0) continue;  // k = 0 excluded (pme.py:435-438)
       double kv[3];
@@ -305,8 +403,8 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
         kv[e] = 2.0 * kPi * (a0 * g.binv[0 * 3 + e] + a1 * g.binv[1 * 3 + e] + a2 * g.binv[2 * 3 + e]);
       const double ksq = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
       const double G = pref / ksq * exp(-ksq * inv4k2) * inv_th2;
-      Gs += 0.5 * G;
-      const double Ek = 0.5 * w * G * s2;
+      Gs += 0.5 * mult * G;
+      const double Ek = 0.5 * mult * w * G * s2;
       v[0] += Ek;
       // dE/dB[a][e] = sum_k E_k (-(1/(4 kappa^2) + 1/k^2)) 2 k_e 2 pi n_a
       const double f = -4.0 * kPi * (inv4k2 + 1.0 / ksq) * Ek;
@@ -322,6 +420,197 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
     R[x * zb + c] = S;
   }
   block_atomic_sum<10>(v, acc + (size_t)s * kAccStride + kAccErec, red);
+  Cplx<T>* P = fft_lines<T, true>(R, F, nz, K0, 1, zb, W, true);
+  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
+    const int x = idx / nz, c = idx - x * nz;
+    H[(size_t)x * xs + c] = P[x * zb + c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused slab passes (one block per x plane, when a plane fits in shared memory):
+//   fft_slab_fwd: Q[x][y][z] -> z R2C (two real lines per complex FFT) -> y FFT
+//                 -> H[x][y][kz]
+//   fft_slab_inv: H[x][y][kz] -> inverse y FFT -> z C2R -> phi[x][y][z]
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __restrict__ mesh,
+                                                           Cplx<T>* __restrict__ spec, int buf_elems) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s = find_sys<F_Y>(b, blockIdx.x);  // F_Y blocks are remapped to one per x plane
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K1 = d.K1, K2 = d.K2, K2h = d.K2h;
+  const int x = blockIdx.x - d.blk_y;
+  const int np = (K1 + 1) / 2;
+  Cplx<T>* W1 = reinterpret_cast<Cplx<T>*>(smem_raw);
+  Cplx<T>* W2 = W1 + b.maxK1;
+  Cplx<T>* A = W2 + b.maxK2;
+  Cplx<T>* B = A + buf_elems;
+  make_twiddles(W1, K1);
+  make_twiddles(W2, K2);
+  const T* Q = mesh + d.mesh_off + (size_t)x * K1 * K2;
+  for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
+    const int p = idx / K2, t = idx - p * K2;
+    Cplx<T> z;
+    z.x = Q[(size_t)(2 * p) * K2 + t];
+    z.y = 2 * p + 1 < K1 ? Q[(size_t)(2 * p + 1) * K2 + t] : T(0);
+    A[p * K2 + t] = z;
+  }
+  __syncthreads();
+  Cplx<T>* R = fft_lines<T, false>(A, B, np, K2, K2, 1, W2, false);
+  Cplx<T>* U = (R == A) ? B : A;
+  // unpack the two-for-one transforms into U[y][kz]
+  for (int idx = threadIdx.x; idx < np * K2h; idx += blockDim.x) {
+    const int p = idx / K2h, k = idx - p * K2h;
+    const Cplx<T> Z = R[p * K2 + k];
+    const Cplx<T> Zm = R[p * K2 + (k == 0 ? 0 : K2 - k)];
+    Cplx<T> a, c;
+    a.x = (Z.x + Zm.x) * T(0.5);
+    a.y = (Z.y - Zm.y) * T(0.5);
+    c.x = (Z.y + Zm.y) * T(0.5);
+    c.y = (Zm.x - Z.x) * T(0.5);
+    U[(2 * p) * K2h + k] = a;
+    if (2 * p + 1 < K1) U[(2 * p + 1) * K2h + k] = c;
+  }
+  __syncthreads();
+  Cplx<T>* V = fft_lines<T, true>(U, R, K2h, K1, 1, K2h, W1, false);
+  Cplx<T>* H = spec + d.spec_off + (size_t)x * K1 * K2h;
+  for (int idx = threadIdx.x; idx < K1 * K2h; idx += blockDim.x) H[idx] = V[idx];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T>* __restrict__ spec,
+                                                           T* __restrict__ mesh, int buf_elems) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s = find_sys<F_Y>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K1 = d.K1, K2 = d.K2, K2h = d.K2h;
+  const int x = blockIdx.x - d.blk_y;
+  const int np = (K1 + 1) / 2;
+  Cplx<T>* W1 = reinterpret_cast<Cplx<T>*>(smem_raw);
+  Cplx<T>* W2 = W1 + b.maxK1;
+  Cplx<T>* A = W2 + b.maxK2;
+  Cplx<T>* B = A + buf_elems;
+  make_twiddles(W1, K1);
+  make_twiddles(W2, K2);
+  const Cplx<T>* H = spec + d.spec_off + (size_t)x * K1 * K2h;
+  for (int idx = threadIdx.x; idx < K1 * K2h; idx += blockDim.x) A[idx] = H[idx];
+  __syncthreads();
+  Cplx<T>* V = fft_lines<T, true>(A, B, K2h, K1, 1, K2h, W1, true);
+  Cplx<T>* Z = (V == A) ? B : A;
+  for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
+    const int p = idx / K2, t = idx - p * K2;
+    const bool lo = t < K2h;
+    const int tt = lo ? t : K2 - t;
+    Cplx<T> a = V[(2 * p) * K2h + tt];
+    Cplx<T> c;
+    if (2 * p + 1 < K1) {
+      c = V[(2 * p + 1) * K2h + tt];
+    } else {
+      c.x = T(0);
+      c.y = T(0);
+    }
+    if (!lo) {
+      a.y = -a.y;
+      c.y = -c.y;
+    }
+    Cplx<T> z;
+    z.x = a.x - c.y;
+    z.y = a.y + c.x;
+    Z[p * K2 + t] = z;
+  }
+  __syncthreads();
+  Cplx<T>* R = fft_lines<T, false>(Z, V, np, K2, K2, 1, W2, true);
+  T* M = mesh + d.mesh_off + (size_t)x * K1 * K2;
+  for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
+    const int p = idx / K2, t = idx - p * K2;
+    const Cplx<T> z = R[p * K2 + t];
+    M[(size_t)(2 * p) * K2 + t] = z.x;
+    if (2 * p + 1 < K1) M[(size_t)(2 * p + 1) * K2 + t] = z.y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cached Green's function for repeated matvecs (CG): green = 2 G_s over the
+// half spectrum, with G_s symmetrised over the reference's mirror labels as in
+// fft_x_green_kernel.  Box and mesh are fixed during a solve.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) green_build_kernel(Batch b, const T* __restrict__ box, T* __restrict__ green,
+                                                          double ke) {
+  __shared__ Geom g;
+  const int s = find_sys<F_X>(b, blockIdx.x);
+  const SysDesc& d = b.s[s];
+  const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h, zb = b.zb;
+  const int ncb = (K2h + zb - 1) / zb;
+  const int local = blockIdx.x - d.blk_x;
+  const int y = local / ncb, cb = local - y * ncb;
+  const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  load_geom(box, d.box_idx, &g);
+  __syncthreads();
+  const double inv4k2 = 1.0 / (4.0 * d.kappa * d.kappa);
+  const double pref = ke * 2.0 * kPi / g.vol;
+  const int ny = signed_k(y, K1), nyb = signed_k(y == 0 ? 0 : K1 - y, K1);
+  const double thy = theta_1d(ny, K1);
+  T* G = green + d.green_off + (size_t)y * K2h + kz0;
+  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
+    const int x = idx / nz, c = idx - x * nz, kz = kz0 + c;
+    const int n0 = signed_k(x, K0), n2 = signed_k(kz, K2);
+    const int n0b = signed_k(x == 0 ? 0 : K0 - x, K0), n2b = signed_k(kz == 0 ? 0 : K2 - kz, K2);
+    const double th = theta_1d(n0, K0) * thy * theta_1d(n2, K2);
+    const bool same = (n0b == -n0) && (nyb == -ny) && (n2b == -n2);
+    double Gs = 0.0;
+    for (int m = 0; m < 2; ++m) {
+      if (m == 1 && same) break;
+      const int a0 = m ? n0b : n0, a1 = m ? nyb : ny, a2 = m ? n2b : n2;
+      if (a0 == 0 && a1 == 0 && a2 == 0) continue;
+      double kv[3];
+      for (int e = 0; e < 3; ++e)
+        kv[e] = 2.0 * kPi * (a0 * g.binv[0 * 3 + e] + a1 * g.binv[1 * 3 + e] + a2 * g.binv[2 * 3 + e]);
+      const double ksq = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+      Gs += (same ? 1.0 : 0.5) * pref / ksq * exp(-ksq * inv4k2) / (th * th);
+    }
+    G[(size_t)x * K1 * K2h + c] = (T)(2.0 * Gs);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fft_x_apply_kernel(Batch b, Cplx<T>* __restrict__ spec,
+                                                          const T* __restrict__ green) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s = find_sys<F_X>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K0 = d.K0, K1 = d.K1, K2h = d.K2h, zb = b.zb;
+  const int ncb = (K2h + zb - 1) / zb;
+  const int local = blockIdx.x - d.blk_x;
+  const int y = local / ncb, cb = local - y * ncb;
+  const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
+  Cplx<T>* A = W + b.maxK0;
+  Cplx<T>* B = A + (size_t)zb * b.maxK0;
+  make_twiddles(W, K0);
+  Cplx<T>* H = spec + d.spec_off + (size_t)y * K2h + kz0;
+  const T* G = green + d.green_off + (size_t)y * K2h + kz0;
+  const size_t xs = (size_t)K1 * K2h;
+  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
+    const int x = idx / nz, c = idx - x * nz;
+    A[x * zb + c] = H[(size_t)x * xs + c];
+  }
+  __syncthreads();
+  Cplx<T>* R = fft_lines<T, true>(A, B, nz, K0, 1, zb, W, false);
+  Cplx<T>* F = (R == A) ? B : A;
+  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
+    const int x = idx / nz, c = idx - x * nz;
+    const T gm = G[(size_t)x * xs + c];
+    Cplx<T> v = R[x * zb + c];
+    v.x *= gm;
+    v.y *= gm;
+    R[x * zb + c] = v;
+  }
+  __syncthreads();
   Cplx<T>* P = fft_lines<T, true>(R, F, nz, K0, 1, zb, W, true);
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
     const int x = idx / nz, c = idx - x * nz;
@@ -382,7 +671,7 @@ __global__ void __launch_bounds__(256) fft_z_inv_kernel(Batch b, const Cplx<T>* 
 }
 
 // ---------------------------------------------------------------------------
-// gather: warp per atom.  pot_i = sum phi theta; dE/du_d = q sum phi dtheta/du_d
+// gather: pot_i = sum phi theta; dE/du_d = q sum phi dtheta/du_d (warp-cooperative)
 // ---------------------------------------------------------------------------
 template <typename T, bool FORCES>
 __global__ void __launch_bounds__(256) gather_kernel(Batch b, const T* __restrict__ pos,
@@ -390,7 +679,9 @@ __global__ void __launch_bounds__(256) gather_kernel(Batch b, const T* __restric
                                                      const T* __restrict__ q,
                                                      const T* __restrict__ phi,
                                                      T* __restrict__ dE_dq, T* __restrict__ dE_dpos,
-                                                     double* __restrict__ acc, T pot_scale) {
+                                                     double* __restrict__ acc, T pot_scale,
+                                                     const int* __restrict__ order) {
+  extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ Geom g;
   __shared__ double red[9 * 32];
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
@@ -399,56 +690,82 @@ __global__ void __launch_bounds__(256) gather_kernel(Batch b, const T* __restric
   load_geom(box, d.box_idx, &g);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
   const int a_begin = (blockIdx.x - d.blk_atom) * b.apb;
   const int a_end = min(a_begin + b.apb, d.natoms);
   const T* M = phi + d.mesh_off;
   const int K[3] = {d.K0, d.K1, d.K2};
+  WarpStencil<T, FORCES> ws;
+  ws.carve(dsm + warp * WarpStencil<T, FORCES>::bytes());
+  const int y0 = lane / 6, z0 = lane % 6, y1 = (lane + 32) / 6, z1 = (lane + 32) % 6;
   double wf[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) wf[k] = 0.0;
-  for (int a = a_begin + warp; a < a_end; a += blockDim.x >> 5) {
-    const int ga = d.atom_off + a;
-    T r[3] = {pos[3 * (size_t)ga], pos[3 * (size_t)ga + 1], pos[3 * (size_t)ga + 2]};
-    Stencil<T> st;
-    make_stencil<T>(r, g, d.K0, d.K1, d.K2, st);
-    T pot = 0, g0 = 0, g1 = 0, g2 = 0;
-    for (int p = lane; p < kStencil; p += 32) {
-      const int dx = p / 36, dy = (p / 6) % 6, dz = p % 6;
-      const size_t idx = ((size_t)st.ix[dx] * d.K1 + st.iy[dy]) * d.K2 + st.iz[dz];
-      const T f = M[idx];
-      const T wyz = st.w[1][dy] * st.w[2][dz];
-      pot += f * st.w[0][dx] * wyz;
+  for (int a0 = a_begin + warp * 32; a0 < a_end; a0 += nw * 32) {
+    warp_build_stencil<T, FORCES>(ws, d, g, pos, FORCES ? q : nullptr, order, a0, a_end, lane);
+    const int na = min(32, a_end - a0);
+    T my_pot = 0, my_g0 = 0, my_g1 = 0, my_g2 = 0;
+    for (int j = 0; j < na; ++j) {
+      const T* w = ws.w + j * 18;
+      const int* ox = ws.ox + j * 6;
+      const int by = ws.byz[2 * j], bz = ws.byz[2 * j + 1];
+      T pot = 0, g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (h == 1 && lane >= 4) break;
+        const int yy = h ? y1 : y0, zz = h ? z1 : z0;
+        const T wy = w[6 + yy], wz = w[12 + zz];
+        const int oyz = wrap_up(by + yy, d.K1) * d.K2 + wrap_up(bz + zz, d.K2);
+        T sw = 0, sdw = 0;
+#pragma unroll
+        for (int dx = 0; dx < 6; ++dx) {
+          const T f = M[ox[dx] + oyz];
+          sw += f * w[dx];
+          if (FORCES) sdw += f * ws.dw[j * 18 + dx];
+        }
+        pot += sw * wy * wz;
+        if (FORCES) {
+          g0 += sdw * wy * wz;
+          g1 += sw * ws.dw[j * 18 + 6 + yy] * wz;
+          g2 += sw * wy * ws.dw[j * 18 + 12 + zz];
+        }
+      }
+      pot = warp_sum(pot);
       if (FORCES) {
-        g0 += f * st.dw[0][dx] * wyz;
-        g1 += f * st.w[0][dx] * st.dw[1][dy] * st.w[2][dz];
-        g2 += f * st.w[0][dx] * st.w[1][dy] * st.dw[2][dz];
+        g0 = warp_sum(g0);
+        g1 = warp_sum(g1);
+        g2 = warp_sum(g2);
+      }
+      if (lane == j) {
+        my_pot = pot;
+        my_g0 = g0;
+        my_g1 = g1;
+        my_g2 = g2;
       }
     }
-    pot = warp_sum(pot);
-    if (FORCES) {
-      g0 = warp_sum(g0);
-      g1 = warp_sum(g1);
-      g2 = warp_sum(g2);
-    }
-    if (lane == 0) {
-      if (dE_dq) dE_dq[ga] += pot * pot_scale;
+    if (lane < na) {
+      const int ga = ws.atom[lane];
+      if (dE_dq) dE_dq[ga] += my_pot * pot_scale;
       if (FORCES) {
-        const T qa = q[ga];
+        const T qa = ws.q[lane];
         // u = m0 - x + 3  ->  dE/dx_d = -q * dE/du_d ; x_d = K_d (r @ B)_d
-        const double gx[3] = {-(double)qa * g0 * K[0], -(double)qa * g1 * K[1], -(double)qa * g2 * K[2]};
+        const double gx[3] = {-(double)qa * my_g0 * K[0], -(double)qa * my_g1 * K[1], -(double)qa * my_g2 * K[2]};
         if (dE_dpos) {
 #pragma unroll
           for (int e = 0; e < 3; ++e) {
-            double v = gx[0] * g.binv[e * 3 + 0] + gx[1] * g.binv[e * 3 + 1] + gx[2] * g.binv[e * 3 + 2];
+            const double v = gx[0] * g.binv[e * 3 + 0] + gx[1] * g.binv[e * 3 + 1] + gx[2] * g.binv[e * 3 + 2];
             dE_dpos[3 * (size_t)ga + e] += (T)v;
           }
         }
+        const double r[3] = {(double)pos[3 * (size_t)ga], (double)pos[3 * (size_t)ga + 1],
+                             (double)pos[3 * (size_t)ga + 2]};
 #pragma unroll
         for (int e = 0; e < 3; ++e)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) wf[e * 3 + c] += (double)r[e] * gx[c];
+          for (int c = 0; c < 3; ++c) wf[e * 3 + c] += r[e] * gx[c];
       }
     }
+    __syncwarp();
   }
   if (FORCES) block_atomic_sum<9>(wf, acc + (size_t)s * kAccStride + kAccWf, red);
 }

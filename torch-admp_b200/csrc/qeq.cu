@@ -11,6 +11,7 @@ struct QEqWS {
   RecipPlan<T> plan;
   T* mesh;
   Cplx<T>* spec;
+  T* green;
   double* acc;
   double *x, *r, *diag, *zc, *chi_eff, *hx;
   T *p, *Hp, *coef;
@@ -32,6 +33,7 @@ static int qeq_carve(QEqWS<T>& w, void* ws, size_t bytes, int N, long long P, co
   Carver c(ws, bytes);
   w.mesh = c.take<T>((flags & ADMP_QEQ_KSPACE) ? w.plan.mesh_elems : 0);
   w.spec = c.take<Cplx<T>>((flags & ADMP_QEQ_KSPACE) ? w.plan.spec_elems : 0);
+  w.green = c.take<T>((flags & ADMP_QEQ_KSPACE) ? w.plan.spec_elems : 0);
   w.acc = c.take<double>(kAccStride);
   w.x = c.take<double>(N);
   w.r = c.take<double>(N);
@@ -67,7 +69,8 @@ template <typename T>
 static int qeq_matvec(QEqCtx<T>& c, const T* v, T* Hv, double* hv_out) {
   const Batch& b = c.w.plan.b;
   if (c.P.flags & ADMP_QEQ_KSPACE) {
-    int s = launch_recip_potential<T>(c.w.plan, c.pos, c.box, v, c.w.mesh, c.w.spec, c.w.acc, c.P.ke, Hv, c.st);
+    int s = launch_recip_potential<T>(c.w.plan, c.pos, c.box, v, c.w.mesh, c.w.spec, c.w.acc, c.P.ke, Hv, c.st,
+                                      nullptr, c.w.green);
     if (s) return s;
   }
   if (c.Pn > 0 && (c.P.flags & (ADMP_QEQ_RSPACE | ADMP_QEQ_DAMPING))) {
@@ -89,6 +92,10 @@ static int qeq_prepare(QEqCtx<T>& c, const T* chi, const T* hard, const T* eta, 
   ADMP_CUDA_TRY(cudaMemsetAsync(c.w.Hp, 0, sizeof(T) * c.N, c.st));
   qeq_setup_kernel<T><<<b.nblk_atom, 256, 0, c.st>>>(b, c.P, c.pos, c.box, chi, hard, eta, shift, c.w.diag, c.w.zc,
                                                     c.w.chi_eff, c.w.sc);
+  if (c.P.flags & ADMP_QEQ_KSPACE) {
+    int s = launch_green_build<T>(c.w.plan, c.box, c.w.green, c.P.ke, c.st);
+    if (s) return s;
+  }
   if (c.nc > 0) {
     qeq_gram_kernel<T><<<b.nblk_atom, 256, 0, c.st>>>(b, c.nc, c.C, (long long)c.N, c.w.sc);
     qeq_gram_invert_kernel<<<1, 32, 0, c.st>>>(b, c.nc, c.w.sc);

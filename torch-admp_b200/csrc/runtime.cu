@@ -1,4 +1,7 @@
 // Status strings, last-error messages and the device error word.
+#include <map>
+#include <mutex>
+#include <utility>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -15,6 +18,20 @@ static bool g_sync = true;
 static DevError* g_err_ptr[64] = {nullptr};
 
 bool sync_checks() { return g_sync; }
+
+// (kernel, device) -> largest dynamic shared memory limit already set
+static std::mutex g_smem_mu;
+static std::map<std::pair<const void*, int>, size_t> g_smem_set;
+
+bool smem_already(const void* fn, size_t bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_smem_mu);
+  size_t& v = g_smem_set[std::make_pair(fn, dev)];
+  if (v >= bytes) return true;
+  v = bytes;
+  return false;
+}
 
 static long long g_launches = 0;
 void count_launches(int n) { g_launches += n; }

@@ -50,10 +50,13 @@ struct Carver {
   bool ok() const { return off <= cap; }
 };
 
-// Sets the max dynamic smem of a kernel once.
+// Raises a kernel's dynamic shared-memory limit to `bytes` (static shared
+// memory counts against the default 48 KB too, so the limit is always set);
+// remembers the largest value set per kernel and device.
+bool smem_already(const void* fn, size_t bytes);
 template <typename K>
 inline cudaError_t ensure_smem(K kernel, size_t bytes) {
-  if (bytes <= 48 * 1024) return cudaSuccess;
+  if (bytes == 0 || smem_already((const void*)kernel, bytes)) return cudaSuccess;
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 

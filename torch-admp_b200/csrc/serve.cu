@@ -119,6 +119,12 @@ static int srv_build(const admp_pools* P, const admp_sys* sys, int nsys, RecipPl
     for (int d = 0; d < 3; ++d) spec[s].K[d] = a.kmesh[d];
     spec[s].kappa = a.kappa;
     spec[s].box_idx = a.slot;
+    spec[s].green_off = a.kind == ADMP_SYS_QEQ ? a.green_off : -1;
+    if (a.kind == ADMP_SYS_QEQ && P->green) {
+      const long long need = (long long)a.kmesh[0] * a.kmesh[1] * (a.kmesh[2] / 2 + 1);
+      if (a.green_off < 0 || a.green_off + need > P->green_cap)
+        return fail(ADMP_ERR_WORKSPACE, "serve: green region of system %d outside the pool", s);
+    }
     c.L.pair_off[s] = a.pair_off;
     c.L.pair_cap[s] = a.pair_cap;
     c.L.rc[s] = a.rcut;
@@ -149,6 +155,7 @@ static int serve_neighbors_impl(const admp_pools* P, const admp_sys* sys, int ns
   SrvSys* ss = (SrvSys*)P->sys_scratch;
   const Batch& b = plan.b;
   typedef typename Vec4<T>::type V4;
+  const int hn = prof_begin(st);
   srv_table_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(c.L, P->box, sizeof(T) == 8, nullptr, ss, 1);
   if (P->pos64 && !P->frac64) return fail(ADMP_ERR_BAD_ARG, "serve: pos64 needs a frac64 scratch");
   const double4* f64 = P->pos64 ? (const double4*)P->frac64 : nullptr;
@@ -162,6 +169,7 @@ static int serve_neighbors_impl(const admp_pools* P, const admp_sys* sys, int ns
   sn_scan_rows_kernel<<<nsys, 1024, 0, st>>>(b, ss, P->pcnt, P->pstart, P->slot_info);
   sn_pairs_kernel<T, true><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, f64, P->cell_of, P->cells,
                                                         P->sorted, P->pcnt, P->pstart, P->col);
+  prof_end(hn, PK_NEIGHBORS, -1.0, st);
   count_launches(8);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
@@ -179,13 +187,15 @@ static int serve_ef_impl(const admp_pools* P, const admp_sys* sys, int nsys, dou
   srv_table_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(c.L, P->box, sizeof(T) == 8, P->slot_info, ss, 0);
   zero_atoms_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, (T*)P->force, P->energy);
   int h = prof_begin(st);
-  pair_ef_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, (const T*)P->q, (const T*)P->eta,
-                                                 P->pstart, P->pcnt, P->col, ke, (T*)P->force, P->energy);
+  pair_ef_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac,
+                                                 P->pos64 ? (const double4*)P->frac64 : nullptr, (const T*)P->q,
+                                                 (const T*)P->eta, P->pstart, P->pcnt, P->col, ke, (T*)P->force,
+                                                 P->energy);
   prof_end(h, PK_PAIR_EF, plan_atoms(plan) * (sizeof(V4) + 2 * sizeof(T) + 12 + 3 * sizeof(T)), st);
   count_launches(6);
   ADMP_CUDA_TRY(cudaMemsetAsync(P->acc, 0, sizeof(double) * kAccStride * nsys, st));
   s = launch_recip<T>(plan, (const T*)P->pos, (const T*)P->box, (const T*)P->q, (T*)P->mesh, (Cplx<T>*)P->spec,
-                      P->acc, ke, nullptr, (T*)P->force, st);
+                      P->acc, ke, nullptr, (T*)P->force, st, P->sorted);
   if (s) return s;
   recip_finalize_kernel<T><<<(nsys + 127) / 128, 128, 0, st>>>(b, (const T*)P->box, P->acc, P->energy, nullptr);
   sys_terms_kernel<T><<<nsys, 512, 0, st>>>(b, ss, (const T*)P->q, (const T*)P->chi, (const T*)P->hardness,
@@ -201,7 +211,7 @@ static int srv_matvec(const admp_pools* P, const RecipPlan<T>& plan, QEqParams p
                       double* hv_out, double ke, cudaStream_t st) {
   const Batch& b = plan.b;
   int s = launch_recip_potential<T>(plan, (const T*)P->pos, (const T*)P->box, v, (T*)P->mesh, (Cplx<T>*)P->spec,
-                                    P->acc, ke, Hv, st);
+                                    P->acc, ke, Hv, st, P->sorted, (const T*)P->green);
   if (s) return s;
   int h = prof_begin(st);
   csr_spmv_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->pstart, P->pcnt, P->col, (const T*)P->coef, v, Hv, b.done,
@@ -241,6 +251,10 @@ static int serve_qeq_init_impl(const admp_pools* P, const admp_sys* sys, int nsy
   qeq_setup_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, (const T*)P->pos, (const T*)P->box, (const T*)P->chi,
                                                   (const T*)P->hardness, (const T*)P->eta, (const T*)nullptr,
                                                   P->cg_diag, P->cg_z, P->cg_chi, sc);
+  if (P->green) {
+    s = launch_green_build<T>(plan, (const T*)P->box, (T*)P->green, ke, st);
+    if (s) return s;
+  }
   // total-charge constraint: Gram = N
   qeq_gram_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, 1, (const T*)nullptr, 0, sc);
   qeq_gram_invert_kernel<<<(nsys + 31) / 32, 32, 0, st>>>(b, 1, sc);
@@ -287,9 +301,11 @@ static int serve_qeq_iterate_impl(const admp_pools* P, const admp_sys* sys, int 
     qeq_rotate_kernel<<<(nsys + 31) / 32, 32, 0, st>>>(b, sc);
     s = srv_matvec<T>(P, plan, prm, (const T*)P->cg_p, (T*)P->cg_hp, nullptr, ke, st);
     if (s) return s;
+    const int hv = prof_begin(st);
     qeq_update_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_x, P->cg_r, (const T*)P->cg_p, (T*)P->cg_hp,
                                                       (const T*)nullptr, 0, sc);
     qeq_direction_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, P->cg_r, (T*)P->cg_p, P->cg_z, sc);
+    prof_end(hv, PK_CG_VECTOR, -1.0, st);
   }
   slot_export_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc, P->slot_info);
   count_launches(1);

@@ -317,9 +317,9 @@ __device__ __forceinline__ void disp(const V4& fi, const V4& fj, const double* b
 template <typename T>
 static __global__ void __launch_bounds__(256)
     pair_ef_kernel(Batch b, const SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
-                   const T* __restrict__ q, const T* __restrict__ eta, const long long* __restrict__ pstart,
-                   const int* __restrict__ pcnt, const int* __restrict__ col, double ke, T* __restrict__ grad,
-                   double* __restrict__ energy) {
+                   const double4* __restrict__ frac64, const T* __restrict__ q, const T* __restrict__ eta,
+                   const long long* __restrict__ pstart, const int* __restrict__ pcnt, const int* __restrict__ col,
+                   double ke, T* __restrict__ grad, double* __restrict__ energy) {
   __shared__ double bx[9];
   __shared__ double red[32];
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
@@ -338,6 +338,7 @@ static __global__ void __launch_bounds__(256)
     for (int a = a0 + warp; a < a1; a += blockDim.x >> 5) {
       const int i = d.atom_off + a;
       const typename Vec4<T>::type fi = frac[i];
+      const double4 fi64 = frac64 ? frac64[i] : make_double4(0, 0, 0, 0);
       const T qi = q[i];
       const T ei = damp ? eta[i] : T(0);
       const long long st = pstart[i];
@@ -345,9 +346,17 @@ static __global__ void __launch_bounds__(256)
       T g0 = 0, g1 = 0, g2 = 0, e = 0;
       for (int k = lane; k < n; k += 32) {
         const int j = col[st + k];
-        const typename Vec4<T>::type fj = frac[j];
         T dr[3];
-        disp(fi, fj, bx, dr);
+        if (frac64) {
+          // displacement from double coordinates: close pairs keep full relative precision
+          double d64[3];
+          disp(fi64, frac64[j], bx, d64);
+          dr[0] = (T)d64[0];
+          dr[1] = (T)d64[1];
+          dr[2] = (T)d64[2];
+        } else {
+          disp(fi, frac[j], bx, dr);
+        }
         const T r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
         const T r = sqrt_t(r2);
         const T inv = T(1) / r;

@@ -261,6 +261,7 @@ __global__ void __launch_bounds__(256) fft_z_fwd_kernel(Batch b, const T* __rest
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
   const int K2 = d.K2, K2h = d.K2h, L = d.K0 * d.K1, npair = (L + 1) / 2;
+  const FastDiv fdK2 = fast_div(K2), fdK2h = fast_div(K2h);
   const int p0 = (blockIdx.x - d.blk_z) * b.lp;
   const int np = min(b.lp, npair - p0);
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
@@ -269,7 +270,7 @@ __global__ void __launch_bounds__(256) fft_z_fwd_kernel(Batch b, const T* __rest
   make_twiddles(W, K2);
   const T* Q = mesh + d.mesh_off;
   for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
-    const int p = idx / K2, t = idx - p * K2;
+    const int p = fdiv(idx, fdK2), t = idx - p * K2;
     const int l0 = 2 * (p0 + p), l1 = l0 + 1;
     Cplx<T> z;
     z.x = Q[(size_t)l0 * K2 + t];
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(256) fft_z_fwd_kernel(Batch b, const T* __rest
   Cplx<T>* R = fft_lines<T, false>(A, B, np, K2, K2, 1, W, false);
   Cplx<T>* H = spec + d.spec_off;
   for (int idx = threadIdx.x; idx < np * K2h; idx += blockDim.x) {
-    const int p = idx / K2h, k = idx - p * K2h;
+    const int p = fdiv(idx, fdK2h), k = idx - p * K2h;
     const Cplx<T> Z = R[p * K2 + k];
     const Cplx<T> Zm = R[p * K2 + (k == 0 ? 0 : K2 - k)];
     const int l0 = 2 * (p0 + p);
@@ -308,19 +309,20 @@ __global__ void __launch_bounds__(256) fft_y_kernel(Batch b, Cplx<T>* __restrict
   const int local = blockIdx.x - d.blk_y;
   const int x = local / ncb, cb = local - x * ncb;
   const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  const FastDiv fdnz = fast_div(nz);
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
   Cplx<T>* A = W + b.maxK1;
   Cplx<T>* B = A + (size_t)zb * b.maxK1;
   make_twiddles(W, K1);
   Cplx<T>* H = spec + d.spec_off + (size_t)x * K1 * K2h + kz0;
   for (int idx = threadIdx.x; idx < K1 * nz; idx += blockDim.x) {
-    const int y = idx / nz, c = idx - y * nz;
+    const int y = fdiv(idx, fdnz), c = idx - y * nz;
     A[y * zb + c] = H[(size_t)y * K2h + c];
   }
   __syncthreads();
   Cplx<T>* R = fft_lines<T, true>(A, B, nz, K1, 1, zb, W, INV);
   for (int idx = threadIdx.x; idx < K1 * nz; idx += blockDim.x) {
-    const int y = idx / nz, c = idx - y * nz;
+    const int y = fdiv(idx, fdnz), c = idx - y * nz;
     H[(size_t)y * K2h + c] = R[y * zb + c];
   }
 }
@@ -343,6 +345,7 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
   const int local = blockIdx.x - d.blk_x;
   const int y = local / ncb, cb = local - y * ncb;
   const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  const FastDiv fdnz = fast_div(nz);
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
   Cplx<T>* A = W + b.maxK0;
   Cplx<T>* B = A + (size_t)zb * b.maxK0;
@@ -355,7 +358,7 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
   Cplx<T>* H = spec + d.spec_off + (size_t)y * K2h + kz0;
   const size_t xs = (size_t)K1 * K2h;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = idx / nz, c = idx - x * nz;
+    const int x = fdiv(idx, fdnz), c = idx - x * nz;
     A[x * zb + c] = H[(size_t)x * xs + c];
   }
   __syncthreads();
@@ -373,7 +376,7 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
 #pragma unroll
   for (int k = 0; k < 10; ++k) v[k] = 0.0;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = idx / nz, c = idx - x * nz;
+    const int x = fdiv(idx, fdnz), c = idx - x * nz;
     const int kz = kz0 + c;
     // A half-spectrum entry p stands for p and its mirror pb = -p (mod K); both
     // carry |S|^2 and the reference's own integer labels.  E = sum G(n)|S|^2
@@ -422,7 +425,7 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
   block_atomic_sum<10>(v, acc + (size_t)s * kAccStride + kAccErec, red);
   Cplx<T>* P = fft_lines<T, true>(R, F, nz, K0, 1, zb, W, true);
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = idx / nz, c = idx - x * nz;
+    const int x = fdiv(idx, fdnz), c = idx - x * nz;
     H[(size_t)x * xs + c] = P[x * zb + c];
   }
 }
@@ -441,6 +444,7 @@ __global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __r
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
   const int K1 = d.K1, K2 = d.K2, K2h = d.K2h;
+  const FastDiv fdK2 = fast_div(K2), fdK2h = fast_div(K2h);
   const int x = blockIdx.x - d.blk_y;
   const int np = (K1 + 1) / 2;
   Cplx<T>* W1 = reinterpret_cast<Cplx<T>*>(smem_raw);
@@ -451,7 +455,7 @@ __global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __r
   make_twiddles(W2, K2);
   const T* Q = mesh + d.mesh_off + (size_t)x * K1 * K2;
   for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
-    const int p = idx / K2, t = idx - p * K2;
+    const int p = fdiv(idx, fdK2), t = idx - p * K2;
     Cplx<T> z;
     z.x = Q[(size_t)(2 * p) * K2 + t];
     z.y = 2 * p + 1 < K1 ? Q[(size_t)(2 * p + 1) * K2 + t] : T(0);
@@ -462,7 +466,7 @@ __global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __r
   Cplx<T>* U = (R == A) ? B : A;
   // unpack the two-for-one transforms into U[y][kz]
   for (int idx = threadIdx.x; idx < np * K2h; idx += blockDim.x) {
-    const int p = idx / K2h, k = idx - p * K2h;
+    const int p = fdiv(idx, fdK2h), k = idx - p * K2h;
     const Cplx<T> Z = R[p * K2 + k];
     const Cplx<T> Zm = R[p * K2 + (k == 0 ? 0 : K2 - k)];
     Cplx<T> a, c;
@@ -487,6 +491,7 @@ __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
   const int K1 = d.K1, K2 = d.K2, K2h = d.K2h;
+  const FastDiv fdK2 = fast_div(K2);
   const int x = blockIdx.x - d.blk_y;
   const int np = (K1 + 1) / 2;
   Cplx<T>* W1 = reinterpret_cast<Cplx<T>*>(smem_raw);
@@ -501,7 +506,7 @@ __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T
   Cplx<T>* V = fft_lines<T, true>(A, B, K2h, K1, 1, K2h, W1, true);
   Cplx<T>* Z = (V == A) ? B : A;
   for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
-    const int p = idx / K2, t = idx - p * K2;
+    const int p = fdiv(idx, fdK2), t = idx - p * K2;
     const bool lo = t < K2h;
     const int tt = lo ? t : K2 - t;
     Cplx<T> a = V[(2 * p) * K2h + tt];
@@ -525,7 +530,7 @@ __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T
   Cplx<T>* R = fft_lines<T, false>(Z, V, np, K2, K2, 1, W2, true);
   T* M = mesh + d.mesh_off + (size_t)x * K1 * K2;
   for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
-    const int p = idx / K2, t = idx - p * K2;
+    const int p = fdiv(idx, fdK2), t = idx - p * K2;
     const Cplx<T> z = R[p * K2 + t];
     M[(size_t)(2 * p) * K2 + t] = z.x;
     if (2 * p + 1 < K1) M[(size_t)(2 * p + 1) * K2 + t] = z.y;
@@ -548,6 +553,7 @@ __global__ void __launch_bounds__(256) green_build_kernel(Batch b, const T* __re
   const int local = blockIdx.x - d.blk_x;
   const int y = local / ncb, cb = local - y * ncb;
   const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  const FastDiv fdnz = fast_div(nz);
   load_geom(box, d.box_idx, &g);
   __syncthreads();
   const double inv4k2 = 1.0 / (4.0 * d.kappa * d.kappa);
@@ -556,7 +562,7 @@ __global__ void __launch_bounds__(256) green_build_kernel(Batch b, const T* __re
   const double thy = theta_1d(ny, K1);
   T* G = green + d.green_off + (size_t)y * K2h + kz0;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = idx / nz, c = idx - x * nz, kz = kz0 + c;
+    const int x = fdiv(idx, fdnz), c = idx - x * nz, kz = kz0 + c;
     const int n0 = signed_k(x, K0), n2 = signed_k(kz, K2);
     const int n0b = signed_k(x == 0 ? 0 : K0 - x, K0), n2b = signed_k(kz == 0 ? 0 : K2 - kz, K2);
     const double th = theta_1d(n0, K0) * thy * theta_1d(n2, K2);
@@ -588,6 +594,7 @@ __global__ void __launch_bounds__(256) fft_x_apply_kernel(Batch b, Cplx<T>* __re
   const int local = blockIdx.x - d.blk_x;
   const int y = local / ncb, cb = local - y * ncb;
   const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  const FastDiv fdnz = fast_div(nz);
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
   Cplx<T>* A = W + b.maxK0;
   Cplx<T>* B = A + (size_t)zb * b.maxK0;
@@ -596,14 +603,14 @@ __global__ void __launch_bounds__(256) fft_x_apply_kernel(Batch b, Cplx<T>* __re
   const T* G = green + d.green_off + (size_t)y * K2h + kz0;
   const size_t xs = (size_t)K1 * K2h;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = idx / nz, c = idx - x * nz;
+    const int x = fdiv(idx, fdnz), c = idx - x * nz;
     A[x * zb + c] = H[(size_t)x * xs + c];
   }
   __syncthreads();
   Cplx<T>* R = fft_lines<T, true>(A, B, nz, K0, 1, zb, W, false);
   Cplx<T>* F = (R == A) ? B : A;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = idx / nz, c = idx - x * nz;
+    const int x = fdiv(idx, fdnz), c = idx - x * nz;
     const T gm = G[(size_t)x * xs + c];
     Cplx<T> v = R[x * zb + c];
     v.x *= gm;
@@ -613,7 +620,7 @@ __global__ void __launch_bounds__(256) fft_x_apply_kernel(Batch b, Cplx<T>* __re
   __syncthreads();
   Cplx<T>* P = fft_lines<T, true>(R, F, nz, K0, 1, zb, W, true);
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = idx / nz, c = idx - x * nz;
+    const int x = fdiv(idx, fdnz), c = idx - x * nz;
     H[(size_t)x * xs + c] = P[x * zb + c];
   }
 }
@@ -629,6 +636,7 @@ __global__ void __launch_bounds__(256) fft_z_inv_kernel(Batch b, const Cplx<T>* 
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
   const int K2 = d.K2, K2h = d.K2h, L = d.K0 * d.K1, npair = (L + 1) / 2;
+  const FastDiv fdK2 = fast_div(K2);
   const int p0 = (blockIdx.x - d.blk_z) * b.lp;
   const int np = min(b.lp, npair - p0);
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
@@ -637,7 +645,7 @@ __global__ void __launch_bounds__(256) fft_z_inv_kernel(Batch b, const Cplx<T>* 
   make_twiddles(W, K2);
   const Cplx<T>* H = spec + d.spec_off;
   for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
-    const int p = idx / K2, t = idx - p * K2;
+    const int p = fdiv(idx, fdK2), t = idx - p * K2;
     const int l0 = 2 * (p0 + p), l1 = l0 + 1;
     const bool lo = t < K2h;
     const int tt = lo ? t : K2 - t;
@@ -662,7 +670,7 @@ __global__ void __launch_bounds__(256) fft_z_inv_kernel(Batch b, const Cplx<T>* 
   Cplx<T>* R = fft_lines<T, false>(A, B, np, K2, K2, 1, W, true);
   T* M = mesh + d.mesh_off;
   for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
-    const int p = idx / K2, t = idx - p * K2;
+    const int p = fdiv(idx, fdK2), t = idx - p * K2;
     const int l0 = 2 * (p0 + p), l1 = l0 + 1;
     const Cplx<T> z = R[p * K2 + t];
     M[(size_t)l0 * K2 + t] = z.x;

@@ -161,7 +161,8 @@ static int serve_neighbors_impl(const admp_pools* P, const admp_sys* sys, int ns
   const double4* f64 = P->pos64 ? (const double4*)P->frac64 : nullptr;
   sn_setup_kernel<T><<<nsys, 256, 0, st>>>(b, ss, (const T*)P->box, P->box64, P->cells);
   sn_bin_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const T*)P->pos, P->pos64, (V4*)P->frac,
-                                                P->pos64 ? (double4*)P->frac64 : nullptr, P->cell_of, P->cells);
+                                                P->pos64 ? (double4*)P->frac64 : nullptr, P->cell_of, P->cells,
+                                                P->pcnt);
   sn_scan_cells_kernel<<<nsys, 1024, 0, st>>>(ss, P->cells);
   sn_scatter_kernel<<<b.nblk_atom, 256, 0, st>>>(b, ss, P->cell_of, P->cells, P->sorted);
   sn_pairs_kernel<T, false><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, f64, P->cell_of, P->cells,

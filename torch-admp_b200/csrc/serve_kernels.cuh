@@ -96,7 +96,7 @@ template <typename T>
 static __global__ void __launch_bounds__(256)
     sn_bin_kernel(Batch b, SrvSys* __restrict__ ss, const T* __restrict__ pos, const double* __restrict__ pos64,
                   typename Vec4<T>::type* __restrict__ frac, double4* __restrict__ frac64, int* __restrict__ cell_of,
-                  int* __restrict__ cells) {
+                  int* __restrict__ cells, int* __restrict__ pcnt) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc& d = b.s[s];
   const SrvSys& S = ss[s];
@@ -104,6 +104,7 @@ static __global__ void __launch_bounds__(256)
   const int a1 = min(a0 + b.apb, d.natoms);
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = d.atom_off + a;
+    pcnt[i] = 0;
     if (S.status) {
       cell_of[i] = -1;
       continue;
@@ -190,7 +191,14 @@ __device__ __forceinline__ void sn_offsets(int nc, int* off, int& n) {
   }
 }
 
-// thread per atom; COUNT: pcnt[i]; FILL: col[pstart[i] + k]
+// Thread per binned atom, visited in cell-sorted order so the lanes of a warp
+// share their candidate cells (their candidate loads mostly coalesce or
+// broadcast).  COUNT: pcnt[i]; FILL: col[pstart[i] + k].  Unbinned atoms had
+// pcnt zeroed by sn_bin_kernel.
+// The cutoff decision is the double-precision one (frac64) whenever frac64 is
+// given: candidates are first tested in T with a margin far above T's
+// rounding error of r^2, and only those inside the margin band around rc^2 or
+// the 1e-4 overlap threshold are re-tested in double.
 template <typename T, bool FILL>
 static __global__ void __launch_bounds__(256)
     sn_pairs_kernel(Batch b, const SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
@@ -200,54 +208,81 @@ static __global__ void __launch_bounds__(256)
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc& d = b.s[s];
   const SrvSys& S = ss[s];
-  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
-  const int a1 = min(a0 + b.apb, d.natoms);
-  if (FILL && S.status) return;
+  if (S.status) return;  // sn_bin_kernel left every count of a failed system at zero
   const int n = S.ncells;
   const int* start = cells + S.cell_off + (n + 1);
+  const int nbinned = start[n];
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, nbinned);
   const double rc2 = S.rc * S.rc;
+  const int nc0 = S.nc[0], nc1 = S.nc[1], nc2 = S.nc[2];
+  int o0[3], o1[3], o2[3], n0, n1, n2;
+  sn_offsets(nc0, o0, n0);
+  sn_offsets(nc1, o1, n1);
+  sn_offsets(nc2, o2, n2);
+  T bt[9];
+  double bsum = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    bt[k] = (T)S.b[k];
+    bsum += fabs(S.b[k]);
+  }
+  const T rc2t = (T)rc2;
+  // |r^2_T - r^2| <= 2 r |dr| with |dr| <= (a few ulp of a fraction) * sum |B|
+  const T mg = frac64 ? (T)(1e-3 * rc2 + 1e-5 * S.rc * bsum) : T(0);
+  const T lo = rc2t - mg, hi = rc2t + mg, small = frac64 ? T(2e-3) : T(1e-4);
+  const int* srt = sorted + d.atom_off;
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
-    const int i = d.atom_off + a;
-    const int ci = S.status ? -1 : cell_of[i];
-    if (ci < 0) {
-      if (!FILL) pcnt[i] = 0;
-      continue;
-    }
-    const int nc0 = S.nc[0], nc1 = S.nc[1], nc2 = S.nc[2];
+    const int i = srt[a];
+    const int ci = cell_of[i];
     const int c0 = ci / (nc1 * nc2), c1 = (ci / nc2) % nc1, c2 = ci % nc2;
-    int o0[3], o1[3], o2[3], n0, n1, n2;
-    sn_offsets(nc0, o0, n0);
-    sn_offsets(nc1, o1, n1);
-    sn_offsets(nc2, o2, n2);
-    const typename Vec4<T>::type fit = frac[i];
-    const double4 fi = frac64 ? frac64[i] : make_double4(fit.x, fit.y, fit.z, 0.0);
+    const typename Vec4<T>::type fi = frac[i];
     int cnt = 0;
     const long long base = FILL ? pstart[i] : 0;
     for (int ia = 0; ia < n0; ++ia) {
-      const int x = (c0 + o0[ia] + nc0) % nc0;
+      int x = c0 + o0[ia];
+      x = x < 0 ? x + nc0 : (x >= nc0 ? x - nc0 : x);
       for (int ib = 0; ib < n1; ++ib) {
-        const int y = (c1 + o1[ib] + nc1) % nc1;
+        int y = c1 + o1[ib];
+        y = y < 0 ? y + nc1 : (y >= nc1 ? y - nc1 : y);
         for (int ic = 0; ic < n2; ++ic) {
-          const int z = (c2 + o2[ic] + nc2) % nc2;
+          int z = c2 + o2[ic];
+          z = z < 0 ? z + nc2 : (z >= nc2 ? z - nc2 : z);
           const int cc = (x * nc1 + y) * nc2 + z;
-          for (int t = start[cc]; t < start[cc + 1]; ++t) {
-            const int j = sorted[d.atom_off + t];
+          const int t1 = start[cc + 1];
+          for (int t = start[cc]; t < t1; ++t) {
+            const int j = srt[t];
             if (j == i) continue;
-            double4 fj;
-            if (frac64) {
-              fj = frac64[j];
-            } else {
-              const typename Vec4<T>::type t = frac[j];
-              fj = make_double4(t.x, t.y, t.z, 0.0);
-            }
-            double df[3] = {fj.x - fi.x, fj.y - fi.y, fj.z - fi.z};
-            for (int e = 0; e < 3; ++e) df[e] -= floor(df[e] + 0.5);
-            double r2 = 0.0;
+            const typename Vec4<T>::type fj = frac[j];
+            T f0 = fj.x - fi.x, f1 = fj.y - fi.y, f2 = fj.z - fi.z;
+            f0 -= floor(f0 + T(0.5));
+            f1 -= floor(f1 + T(0.5));
+            f2 -= floor(f2 + T(0.5));
+            T r2 = 0;
+#pragma unroll
             for (int e = 0; e < 3; ++e) {
-              const double v = df[0] * S.b[0 * 3 + e] + df[1] * S.b[1 * 3 + e] + df[2] * S.b[2 * 3 + e];
+              const T v = f0 * bt[e] + f1 * bt[3 + e] + f2 * bt[6 + e];
               r2 += v * v;
             }
-            if (r2 < rc2 && r2 > 1e-4) {
+            bool in;
+            if (r2 > hi) {
+              in = false;
+            } else if (r2 < lo && r2 > small) {
+              in = true;
+            } else if (!frac64) {
+              in = r2 < rc2t && r2 > T(1e-4);
+            } else {
+              const double4 gi = frac64[i], gj = frac64[j];
+              double df[3] = {gj.x - gi.x, gj.y - gi.y, gj.z - gi.z};
+              for (int e = 0; e < 3; ++e) df[e] -= floor(df[e] + 0.5);
+              double rr = 0.0;
+              for (int e = 0; e < 3; ++e) {
+                const double v = df[0] * S.b[0 * 3 + e] + df[1] * S.b[1 * 3 + e] + df[2] * S.b[2 * 3 + e];
+                rr += v * v;
+              }
+              in = rr < rc2 && rr > 1e-4;
+            }
+            if (in) {
               if (FILL) col[base + cnt] = j;
               ++cnt;
             }

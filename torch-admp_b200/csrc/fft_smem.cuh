@@ -26,27 +26,23 @@ __device__ __forceinline__ void factor_radices(int n, Radices& R) {
   if (m > 1) R.r[R.ns++] = m;
 }
 
-// Division by a runtime but block-uniform divisor through a float reciprocal
-// (operands stay far below 2^22, so the estimate is off by at most one and
-// one correction step makes it exact).
+// Division by a runtime but block-uniform divisor without the conversion /
+// reciprocal pipe: q = (x * m) >> 32 with m = ceil(2^32 / d) is exact for
+// 0 <= x < 2^16 and 1 <= d <= 2^16 (the error term x (m - 2^32/d) / 2^32 stays
+// below 1/d).  Every shared-memory index in these kernels is below 2^16 (a
+// block never holds more than 227 KB / 8 B complex values).
 struct FastDiv {
   int d;
-  float inv;
+  unsigned m;
 };
-__device__ __forceinline__ FastDiv fast_div(int d) {
+__host__ __device__ __forceinline__ FastDiv fast_div(int d) {
   FastDiv f;
   f.d = d;
-  f.inv = 1.0f / (float)d;
+  f.m = d > 1 ? 0xFFFFFFFFu / (unsigned)d + 1u : 0u;
   return f;
 }
 __device__ __forceinline__ int fdiv(int x, const FastDiv& f) {
-  int q = __float2int_rz((float)x * f.inv);
-  const int r = x - q * f.d;
-  if (r < 0)
-    --q;
-  else if (r >= f.d)
-    ++q;
-  return q;
+  return f.d > 1 ? (int)__umulhi((unsigned)x, f.m) : x;
 }
 
 // W[e] = exp(-2 pi i e / n), e in [0, n); computed in double.
@@ -60,45 +56,106 @@ __device__ __forceinline__ void make_twiddles(Cplx<T>* W, int n) {
   }
 }
 
-// One Stockham stage with radix r over nl lines of length n.
-// Element (l, t) lives at buf[l * ls + t * es].
-// LINE_FAST selects the thread mapping (consecutive threads -> consecutive
-// lines, for layouts where the line stride is the unit stride).
+// One Stockham stage with an odd prime radix r >= 7 over nl lines of length n.
+// Element (l, t) lives at buf[l * ls + t * es].  LINE_FAST selects the thread
+// mapping (consecutive threads -> consecutive lines, for layouts where the
+// line stride is the unit stride).
+// The r-point DFT of each butterfly uses the pairing of inputs t and r - t:
+//   X_k     = v_0 + sum_t s_t cos(2 pi t k / r) -/+ i sum_t d_t sin(2 pi t k / r)
+//   X_{r-k} = v_0 + sum_t s_t cos(...)          +/- i sum_t d_t sin(...)
+// with s_t = v_t + v_{r-t}, d_t = v_t - v_{r-t} (t = 1 .. (r-1)/2), which needs
+// about r^2 / 4 complex-by-real products per butterfly instead of r^2 complex
+// ones.  Step 1 twiddles and folds the inputs (in -> out, in the butterfly's
+// own output slots), step 2 forms the output pairs (out -> in), so the result
+// of this stage is left in `in`.
 template <typename T, bool LINE_FAST>
-__device__ __forceinline__ void stockham_stage(const Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
-                                               int nl, int n, int ls, int es, int Ns, int r,
-                                               const Cplx<T>* __restrict__ W, bool inverse) {
-  const int total = nl * n;
-  const int nr = n / r;
+__device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
+                                             int nl, int n, int ls, int es, int Ns, int r,
+                                             const Cplx<T>* __restrict__ W, bool inverse) {
+  const int nb = n / r;
+  const int h = (r - 1) >> 1;
   const int scale = n / (Ns * r);
-  const FastDiv f_split = fast_div(LINE_FAST ? nl : n), f_nsr = fast_div(Ns * r), f_ns = fast_div(Ns);
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+  const int wr = n / r;  // W[e * wr] = exp(-2 pi i e / r)
+  const FastDiv f_split = fast_div(LINE_FAST ? nl : nb), f_ns = fast_div(Ns), f_items = fast_div(nl * nb);
+  const int total1 = nl * nb;
+  for (int idx = threadIdx.x; idx < total1; idx += blockDim.x) {
     const int qd = fdiv(idx, f_split);
     const int rm = idx - qd * f_split.d;
     const int l = LINE_FAST ? rm : qd;
-    const int o = LINE_FAST ? qd : rm;
-    const int q = fdiv(o, f_nsr);
-    const int rem = o - q * (Ns * r);
-    const int u = fdiv(rem, f_ns);
-    const int k = rem - u * Ns;
-    const int j = q * Ns + k;
-    const int c = scale * (k + u * Ns);
-    const Cplx<T>* src = in + (size_t)l * ls + (size_t)j * es;
-    T sx = 0, sy = 0;
-    int e = 0;
-    for (int t = 0; t < r; ++t) {
-      Cplx<T> x = src[(size_t)t * nr * es];
-      Cplx<T> w = W[e];
-      T wy = inverse ? -w.y : w.y;
-      sx += x.x * w.x - x.y * wy;
-      sy += x.x * wy + x.y * w.x;
-      e += c;
-      if (e >= n) e -= n;
+    const int j = LINE_FAST ? qd : rm;
+    const int jq = fdiv(j, f_ns);
+    const int k = j - jq * Ns;
+    const Cplx<T>* src = in + (size_t)l * ls;
+    Cplx<T>* dst = out + (size_t)l * ls;
+    const int base = jq * Ns * r + k;
+    dst[(size_t)base * es] = src[(size_t)j * es];
+    for (int u = 1; u <= h; ++u) {
+      const Cplx<T> a = src[(size_t)(j + u * nb) * es];
+      const Cplx<T> c = src[(size_t)(j + (r - u) * nb) * es];
+      const Cplx<T> wa = W[scale * k * u];
+      const Cplx<T> wc = W[scale * k * (r - u)];
+      const T way = inverse ? -wa.y : wa.y, wcy = inverse ? -wc.y : wc.y;
+      const T ax = a.x * wa.x - a.y * way, ay = a.x * way + a.y * wa.x;
+      const T cx = c.x * wc.x - c.y * wcy, cy = c.x * wcy + c.y * wc.x;
+      Cplx<T> sv, dv;
+      sv.x = ax + cx;
+      sv.y = ay + cy;
+      dv.x = ax - cx;
+      dv.y = ay - cy;
+      dst[(size_t)(base + u * Ns) * es] = sv;
+      dst[(size_t)(base + (h + u) * Ns) * es] = dv;
     }
-    Cplx<T> res;
-    res.x = sx;
-    res.y = sy;
-    out[(size_t)l * ls + (size_t)o * es] = res;
+  }
+  __syncthreads();
+  const int total2 = (h + 1) * total1;
+  for (int idx = threadIdx.x; idx < total2; idx += blockDim.x) {
+    const int kk = fdiv(idx, f_items);
+    const int it = idx - kk * f_items.d;
+    const int qd = fdiv(it, f_split);
+    const int rm = it - qd * f_split.d;
+    const int l = LINE_FAST ? rm : qd;
+    const int j = LINE_FAST ? qd : rm;
+    const int jq = fdiv(j, f_ns);
+    const int k = j - jq * Ns;
+    const Cplx<T>* src = out + (size_t)l * ls;
+    Cplx<T>* dst = in + (size_t)l * ls;
+    const int base = jq * Ns * r + k;
+    const Cplx<T> v0 = src[(size_t)base * es];
+    T ax = v0.x, ay = v0.y;
+    if (kk == 0) {
+      for (int u = 1; u <= h; ++u) {
+        const Cplx<T> sv = src[(size_t)(base + u * Ns) * es];
+        ax += sv.x;
+        ay += sv.y;
+      }
+      Cplx<T> X;
+      X.x = ax;
+      X.y = ay;
+      dst[(size_t)base * es] = X;
+      continue;
+    }
+    T bx = 0, by = 0;
+    int e = 0;
+    for (int u = 1; u <= h; ++u) {
+      e += kk;
+      if (e >= r) e -= r;
+      const Cplx<T> w = W[e * wr];  // (cos, -sin) of 2 pi e / r
+      const Cplx<T> sv = src[(size_t)(base + u * Ns) * es];
+      const Cplx<T> dv = src[(size_t)(base + (h + u) * Ns) * es];
+      ax += sv.x * w.x;
+      ay += sv.y * w.x;
+      bx -= dv.x * w.y;
+      by -= dv.y * w.y;
+    }
+    // forward: X_k = A - i B, X_{r-k} = A + i B (inverse: signs swapped); -i B = (B.y, -B.x)
+    const T ibx = inverse ? -by : by, iby = inverse ? bx : -bx;
+    Cplx<T> X1, X2;
+    X1.x = ax + ibx;
+    X1.y = ay + iby;
+    X2.x = ax - ibx;
+    X2.y = ay - iby;
+    dst[(size_t)(base + kk * Ns) * es] = X1;
+    dst[(size_t)(base + (r - kk) * Ns) * es] = X2;
   }
 }
 
@@ -283,12 +340,14 @@ __device__ Cplx<T>* fft_lines(Cplx<T>* a, Cplx<T>* b, int nl, int n, int ls, int
     else if (r == 5)
       stockham_r35<T, LINE_FAST, 5>(in, out, nl, n, ls, es, Ns, W, inverse);
     else
-      stockham_stage<T, LINE_FAST>(in, out, nl, n, ls, es, Ns, r, W, inverse);
+      stockham_odd<T, LINE_FAST>(in, out, nl, n, ls, es, Ns, r, W, inverse);
     __syncthreads();
     Ns *= r;
-    Cplx<T>* tmp = in;
-    in = out;
-    out = tmp;
+    if (r <= 5) {  // the odd-radix stage leaves its result in `in`
+      Cplx<T>* tmp = in;
+      in = out;
+      out = tmp;
+    }
   }
   return in;
 }

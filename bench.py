@@ -310,6 +310,8 @@ def main():
     st = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches0 = L.launch_count()
+    for k in eng.host_time:
+        eng.host_time[k] = 0.0
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(dev.index) as clk:
@@ -326,6 +328,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     ms_per_step = ms / args.steps
+    host_ms = {k: round(v * 1000.0 / args.steps, 3) for k, v in eng.host_time.items()}
     value = args.nreq * world / (ms_per_step / 1000.0)
     n_bad = sum(1 for r in res if r.status != 0)
 
@@ -422,6 +425,7 @@ def main():
                          "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
                          "kernels": rf},
             "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
+            "host_ms_per_step": host_ms,
             "gpu_launches": int(launches),
             "clocks": clocks,
             "failed_requests": n_bad,

@@ -156,7 +156,7 @@ class ServingEngine:
     def __init__(self, device="cuda:0", dtype=torch.float32, max_atoms: int = 4_000_000, max_slots: int = 512,
                  pairs_per_atom: float = 150.0, mesh_budget: int = 64_000_000, rcut: float = 6.0,
                  ethresh: float = 5e-4, tol: float = 1e-6, max_iter: int = 300, iters_per_tick: int = 8,
-                 ke: float = DIELECTRIC, green_budget: Optional[int] = None):
+                 ke: float = DIELECTRIC, green_budget: Optional[int] = None, admit_per_tick: int = 512):
         self.lib = L.load()
         _bind_serve(self.lib)
         self.dev = torch.device(device)
@@ -166,6 +166,8 @@ class ServingEngine:
         self.kappa = math.sqrt(-math.log(2 * ethresh)) / rcut
         self.tol, self.max_iter, self.iters_per_tick, self.ke = tol, max_iter, iters_per_tick, ke
         self.max_slots = max_slots
+        # admissions per scheduler step: later ones are uploaded while the device works on earlier ones
+        self.admit_per_tick = admit_per_tick
         A = max_atoms
         Pn = int(max_atoms * pairs_per_atom)
         f = dict(dtype=dtype, device=self.dev)
@@ -222,6 +224,11 @@ class ServingEngine:
         self.stream = torch.cuda.current_stream(self.dev)
         self.pin = {}
         self.stats = {"ticks": 0, "launch_calls": 0, "admitted": 0, "h2d_bytes": 0, "d2h_bytes": 0}
+        self._fact_cache: Dict[int, tuple] = {}
+        self._inflight: List[tuple] = []  # launched work whose results are not read yet, in launch order
+        self._zeros = {dt: torch.zeros(3 * 64, dtype=dt, device=self.dev) for dt in (torch.float32, torch.float64)}
+        # host seconds per scheduler phase (admission + upload, launches, waiting on the device, reading results)
+        self.host_time = {"admit": 0.0, "launch": 0.0, "wait": 0.0, "results": 0.0}
         # results as host numpy arrays (True) or device tensors (False)
         self.results_to_host = True
 
@@ -252,6 +259,15 @@ class ServingEngine:
     # -- API ------------------------------------------------------------------
     def submit(self, req, t_arrival: Optional[float] = None) -> None:
         self.queue.append((req, time.perf_counter() if t_arrival is None else t_arrival))
+
+    def _facts(self, req):
+        """(kmesh, mesh elements, pair capacity) of a request, computed once."""
+        f = self._fact_cache.get(id(req))
+        if f is None or f[0] is not req:
+            km = auto_kmesh(np.diagonal(self._box_host(req)), self.kappa, self.ethresh)
+            f = (req, km, self._mesh_of(km), self._pair_estimate(req))
+            self._fact_cache[id(req)] = f
+        return f[1], f[2], f[3]
 
     def _sys_array(self, items: List[_Active]):
         """ctypes array of the launch descriptors; each request's descriptor is
@@ -306,12 +322,11 @@ class ServingEngine:
         admitted = []
         blocked = False
         for req, tarr in ready:
-            if blocked:
+            if blocked or len(admitted) >= self.admit_per_tick:
                 keep.append((req, tarr))
                 continue
             n = req.natoms
-            km = auto_kmesh(np.diagonal(self._box_host(req)), self.kappa, self.ethresh)
-            m = self._mesh_of(km)
+            km, m, pcap = self._facts(req)
             if not self.free_slots or m > self.mesh_budget:
                 keep.append((req, tarr))
                 continue
@@ -319,7 +334,6 @@ class ServingEngine:
             if aoff is None:
                 keep.append((req, tarr))
                 continue
-            pcap = self._pair_estimate(req)
             poff = self.pairs.alloc(pcap)
             if poff is None:
                 self.atoms.release(aoff, n)
@@ -339,34 +353,58 @@ class ServingEngine:
             admitted.append(_Active(req, slot, aoff, poff, pcap, km, kind, tarr, goff, gn))
         keep.sort(key=lambda rt: rt[1])
         self.queue = keep
+        if len(self._fact_cache) > 200_000:
+            self._fact_cache.clear()
         if admitted:
             self._upload(admitted)
             self.stats["admitted"] += len(admitted)
         return admitted
 
-    @staticmethod
-    def _runs(items: List[_Active]):
-        """Maximal runs of items whose atom regions are back to back."""
+    def _runs(self, items: List[_Active]):
+        """Maximal runs of items whose atom regions follow each other up to the
+        allocator's alignment padding."""
+        al = self.atoms.align
         runs, cur = [], []
         for a in items:
-            if cur and cur[-1].atom_off + cur[-1].req.natoms != a.atom_off:
-                runs.append(cur)
-                cur = []
+            if cur:
+                end = cur[-1].atom_off + cur[-1].req.natoms
+                if a.atom_off != (end + al - 1) // al * al:
+                    runs.append(cur)
+                    cur = []
             cur.append(a)
         if cur:
             runs.append(cur)
         return runs
 
-    def _stack(self, arrays, dtype):
-        """Concatenate request arrays into one source tensor: device tensors
-        with torch.cat, host arrays through one pinned buffer.  Returns
+    def _stack(self, arrays, dtype, pads=None, width=1):
+        """Concatenate request arrays into one source tensor, with pads[k] zero
+        rows (of `width` values) after array k: device tensors with one
+        torch.cat, host arrays through one pinned buffer.  Returns
         (tensor, host bytes)."""
+        pads = pads or [0] * len(arrays)
         if isinstance(arrays[0], torch.Tensor):
-            return torch.cat([a.reshape(-1).to(dtype) for a in arrays]), 0
+            # rows of `width` values, concatenated along dim 0 (one batched copy)
+            parts = []
+            zero = self._zeros[dtype]
+            for a, p in zip(arrays, pads):
+                parts.append(a if a.dtype == dtype else a.to(dtype))
+                if p:
+                    parts.append(zero[:p * width].view(p, width) if a.dim() == 2 else zero[:p * width])
+            return (torch.cat(parts) if len(parts) > 1 else parts[0]).reshape(-1), 0
         npdt = {torch.float32: np.float32, torch.float64: np.float64}[dtype]
-        host = np.concatenate([np.asarray(a, dtype=npdt).reshape(-1) for a in arrays])
+        parts = []
+        for a, p in zip(arrays, pads):
+            parts.append(np.asarray(a, dtype=npdt).reshape(-1))
+            if p:
+                parts.append(np.zeros(p * width, dtype=npdt))
+        host = np.concatenate(parts) if len(parts) > 1 else parts[0]
         t = torch.from_numpy(host).pin_memory()
         return t, t.numel() * t.element_size()
+
+    @staticmethod
+    def _pads(run):
+        """Zero rows between consecutive items of a run (alignment padding)."""
+        return [run[k + 1].atom_off - (run[k].atom_off + run[k].req.natoms) for k in range(len(run) - 1)] + [0]
 
     def _upload(self, items: List[_Active]) -> None:
         t = self.t
@@ -383,7 +421,8 @@ class ServingEngine:
             lo = run[0].atom_off
             hi = run[-1].atom_off + run[-1].req.natoms
             sl = slice(lo, hi)
-            pos, b = self._stack([a.req.pos for a in run], torch.float64 if has64 else self.dtype)
+            pads = self._pads(run)
+            pos, b = self._stack([a.req.pos for a in run], torch.float64 if has64 else self.dtype, pads, 3)
             nb += b
             if has64:
                 # positions arrive in double; the FP32 copy is made on the device
@@ -399,13 +438,14 @@ class ServingEngine:
                     j += 1
                 sub = run[k:j]
                 ssl = slice(sub[0].atom_off, sub[-1].atom_off + sub[-1].req.natoms)
+                spads = pads[k:j - 1] + [0]
                 if sub[0].kind == SYS_PME:
-                    q, b = self._stack([a.req.charges for a in sub], self.dtype)
+                    q, b = self._stack([a.req.charges for a in sub], self.dtype, spads)
                     t["q"][ssl].copy_(q, non_blocking=True)
                     nb += b
                 else:
                     for name in ("chi", "hardness", "eta"):
-                        v, b = self._stack([getattr(a.req, name) for a in sub], self.dtype)
+                        v, b = self._stack([getattr(a.req, name) for a in sub], self.dtype, spads)
                         t[name][ssl].copy_(v, non_blocking=True)
                         nb += b
                     t["q"][ssl].zero_()
@@ -419,12 +459,11 @@ class ServingEngine:
                 k = j
         self.stats["h2d_bytes"] += nb
 
-    def _finish(self, items: List[_Active], now_fn) -> None:
-        """Energy + forces of finished systems, results out, resources freed.
-        Forces (and QEq charges) of all finished systems leave the device in
-        one gather + one copy."""
-        if not items:
-            return
+    def _launch_finish(self, items: List[_Active]):
+        """Launch energy + forces of finished systems and the copies of their
+        results (forces and QEq charges of all of them leave the device in one
+        gather + one copy); returns the in-flight record that
+        _complete_finish reads once the record's event has passed."""
         self._call(self.lib.admp_serve_energy_forces, items, self.ke)
         t = self.t
         host = self.results_to_host
@@ -445,23 +484,31 @@ class ServingEngine:
         E.copy_(t["energy"], non_blocking=True)
         info = torch.empty(self.max_slots, 4, dtype=torch.int32, pin_memory=True)
         info.copy_(t["slot_info"], non_blocking=True)
-        self.stream.synchronize()
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        return ("finish", ev, items, runs, qruns, F_all, q_all, E, info)
+
+    def _complete_finish(self, rec, now_fn) -> None:
+        """Results of a finish record out, resources freed (its event has passed)."""
+        _, _, items, runs, qruns, F_all, q_all, E, info = rec
+        host = self.results_to_host
         tdone = now_fn()
         Fsrc = F_all.numpy() if host else F_all
         qsrc = (q_all.numpy() if host else q_all) if q_all is not None else None
         Eh = E.numpy()
         ih = info.numpy()
+        # row of each system inside the gathered arrays (runs keep their alignment padding)
         off, qoff = {}, {}
         o = 0
         for r in runs:
             for a in r:
-                off[a.slot] = o
-                o += a.req.natoms
+                off[a.slot] = o + a.atom_off - r[0].atom_off
+            o += r[-1].atom_off + r[-1].req.natoms - r[0].atom_off
         o = 0
         for r in qruns:
             for a in r:
-                qoff[a.slot] = o
-                o += a.req.natoms
+                qoff[a.slot] = o + a.atom_off - r[0].atom_off
+            o += r[-1].atom_off + r[-1].req.natoms - r[0].atom_off
         for a in items:
             n = a.req.natoms
             Fo = Fsrc[off[a.slot]:off[a.slot] + n]
@@ -475,6 +522,40 @@ class ServingEngine:
             self.results.append(Result(a.req.rid, a.req.kind, float(Eh[a.slot]), Fo, qo, it, st, a.t_arrival, tdone))
             self._release(a)
 
+    def _complete_iterate(self, rec) -> None:
+        """Systems whose done flag (or error) showed in an iterate record's
+        snapshot leave the CG set; their finish work is launched."""
+        _, _, act, info = rec
+        ih = info.numpy()
+        done = [a for a in act if self.active_qeq.get(a.slot) is a and (ih[a.slot, 0] != 0 or ih[a.slot, 2] != 0)]
+        for a in done:
+            del self.active_qeq[a.slot]
+        if done:
+            self._call(self.lib.admp_serve_qeq_finish, done)
+            self._inflight.append(self._launch_finish(done))
+
+    def _drain(self, now_fn, max_iter_records: int) -> None:
+        """Complete in-flight records in launch order: every record whose
+        event has passed, and the oldest ones (waiting on them) while more than
+        `max_iter_records` iterate records are outstanding (all of them when
+        it is 0).  Keeping one iterate record in flight lets the host read
+        results while the device works on the next batch of CG iterations."""
+        while self._inflight:
+            rec = self._inflight[0]
+            n_iter = sum(1 for r in self._inflight if r[0] == "iter")
+            if max_iter_records > 0 and n_iter <= max_iter_records and not rec[1].query():
+                break
+            self._inflight.pop(0)
+            h0 = time.perf_counter()
+            rec[1].synchronize()
+            h1 = time.perf_counter()
+            self.host_time["wait"] += h1 - h0
+            if rec[0] == "finish":
+                self._complete_finish(rec, now_fn)
+            else:
+                self._complete_iterate(rec)
+            self.host_time["results"] += time.perf_counter() - h1
+
     def _release(self, a: _Active) -> None:
         self.atoms.release(a.atom_off, a.req.natoms)
         self.pairs.release(a.pair_off, a.pair_cap)
@@ -483,10 +564,19 @@ class ServingEngine:
         self.free_slots.append(a.slot)
 
     def tick(self, now_fn=time.perf_counter) -> int:
-        """One scheduler step; returns the number of results completed."""
+        """One scheduler step; returns the number of results completed.
+
+        Work is launched first (neighbour lists, CG set-up and PME
+        energy + forces of newly admitted systems, then a batch of CG
+        iterations over every active QEq system with a snapshot of the
+        per-slot done flags); results of earlier steps are read afterwards,
+        so the device stays busy while the host schedules."""
         n0 = len(self.results)
         now = now_fn()
+        h0 = time.perf_counter()
         new = self._admit(now)
+        h1 = time.perf_counter()
+        self.host_time["admit"] += h1 - h0
         if new:
             self._call(self.lib.admp_serve_neighbors, new)
             pme = [a for a in new if a.kind == SYS_PME]
@@ -496,25 +586,22 @@ class ServingEngine:
                 for a in qeq:
                     self.active_qeq[a.slot] = a
             if pme:
-                self._finish(pme, now_fn)
+                self._inflight.append(self._launch_finish(pme))
         if self.active_qeq:
             act = list(self.active_qeq.values())
             self._call(self.lib.admp_serve_qeq_iterate, act, self.iters_per_tick, self.tol, self.max_iter, self.ke)
             info = torch.empty(self.max_slots, 4, dtype=torch.int32, pin_memory=True)
             info.copy_(self.t["slot_info"], non_blocking=True)
-            self.stream.synchronize()
-            ih = info.numpy()
-            done = [a for a in act if ih[a.slot, 0] != 0 or ih[a.slot, 2] != 0]
-            for a in done:
-                del self.active_qeq[a.slot]
-            if done:
-                self._call(self.lib.admp_serve_qeq_finish, done)
-                self._finish(done, now_fn)
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+            self._inflight.append(("iter", ev, act, info))
+        self.host_time["launch"] += time.perf_counter() - h1
+        self._drain(now_fn, 1 if self.active_qeq else 0)
         self.stats["ticks"] += 1
         return len(self.results) - n0
 
     def pending(self) -> int:
-        return len(self.queue) + len(self.active_qeq)
+        return len(self.queue) + len(self.active_qeq) + len(self._inflight)
 
     def run(self, requests, arrivals: bool = True, time_scale: float = 1.0, max_seconds: float = 1e9):
         """Serve a list of requests.  With ``arrivals`` the request ``arrival``
@@ -524,7 +611,7 @@ class ServingEngine:
         for r in requests:
             self.submit(r, t0 + (r.arrival * time_scale if arrivals else 0.0))
         while self.pending():
-            if self.tick() == 0 and not self.active_qeq:
+            if self.tick() == 0 and not self.active_qeq and not self._inflight:
                 # nothing on the device: wait for the next arrival
                 nxt = min(t for _, t in self.queue) if self.queue else None
                 if nxt is not None:

@@ -231,6 +231,11 @@ static __global__ void __launch_bounds__(256)
   // |r^2_T - r^2| <= 2 r |dr| with |dr| <= (a few ulp of a fraction) * sum |B|
   const T mg = frac64 ? (T)(1e-3 * rc2 + 1e-5 * S.rc * bsum) : T(0);
   const T lo = rc2t - mg, hi = rc2t + mg, small = frac64 ? T(2e-3) : T(1e-4);
+  // with >= 3 cells on every axis the image of a candidate is fixed by its
+  // cell's wrap, so no rounding to the nearest image is needed
+  const bool fast = nc0 >= 3 && nc1 >= 3 && nc2 >= 3;
+  const bool ortho = S.b[1] == 0.0 && S.b[2] == 0.0 && S.b[3] == 0.0 && S.b[5] == 0.0 && S.b[6] == 0.0 &&
+                     S.b[7] == 0.0;
   const int* srt = sorted + d.atom_off;
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = srt[a];
@@ -241,28 +246,58 @@ static __global__ void __launch_bounds__(256)
     const long long base = FILL ? pstart[i] : 0;
     for (int ia = 0; ia < n0; ++ia) {
       int x = c0 + o0[ia];
-      x = x < 0 ? x + nc0 : (x >= nc0 ? x - nc0 : x);
+      T s0 = 0;
+      if (x < 0) {
+        x += nc0;
+        s0 = T(-1);
+      } else if (x >= nc0) {
+        x -= nc0;
+        s0 = T(1);
+      }
       for (int ib = 0; ib < n1; ++ib) {
         int y = c1 + o1[ib];
-        y = y < 0 ? y + nc1 : (y >= nc1 ? y - nc1 : y);
+        T s1 = 0;
+        if (y < 0) {
+          y += nc1;
+          s1 = T(-1);
+        } else if (y >= nc1) {
+          y -= nc1;
+          s1 = T(1);
+        }
         for (int ic = 0; ic < n2; ++ic) {
           int z = c2 + o2[ic];
-          z = z < 0 ? z + nc2 : (z >= nc2 ? z - nc2 : z);
+          T s2 = 0;
+          if (z < 0) {
+            z += nc2;
+            s2 = T(-1);
+          } else if (z >= nc2) {
+            z -= nc2;
+            s2 = T(1);
+          }
+          const T g0 = s0 - fi.x, g1 = s1 - fi.y, g2 = s2 - fi.z;
           const int cc = (x * nc1 + y) * nc2 + z;
           const int t1 = start[cc + 1];
           for (int t = start[cc]; t < t1; ++t) {
             const int j = srt[t];
             if (j == i) continue;
             const typename Vec4<T>::type fj = frac[j];
-            T f0 = fj.x - fi.x, f1 = fj.y - fi.y, f2 = fj.z - fi.z;
-            f0 -= floor(f0 + T(0.5));
-            f1 -= floor(f1 + T(0.5));
-            f2 -= floor(f2 + T(0.5));
-            T r2 = 0;
+            T f0 = fj.x + g0, f1 = fj.y + g1, f2 = fj.z + g2;
+            if (!fast) {
+              f0 -= floor(f0 + T(0.5));
+              f1 -= floor(f1 + T(0.5));
+              f2 -= floor(f2 + T(0.5));
+            }
+            T r2;
+            if (ortho) {
+              const T v0 = f0 * bt[0], v1 = f1 * bt[4], v2 = f2 * bt[8];
+              r2 = v0 * v0 + v1 * v1 + v2 * v2;
+            } else {
+              r2 = 0;
 #pragma unroll
-            for (int e = 0; e < 3; ++e) {
-              const T v = f0 * bt[e] + f1 * bt[3 + e] + f2 * bt[6 + e];
-              r2 += v * v;
+              for (int e = 0; e < 3; ++e) {
+                const T v = f0 * bt[e] + f1 * bt[3 + e] + f2 * bt[6 + e];
+                r2 += v * v;
+              }
             }
             bool in;
             if (r2 > hi) {

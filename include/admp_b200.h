@@ -79,7 +79,7 @@ long long admp_launch_count(void);
  * with their algorithmic bytes.  admp_profile_read fills per-kernel totals
  * (index order: spread, fft_z_fwd, fft_y_fwd, fft_x_green, fft_y_inv,
  * fft_z_inv, gather, pair_ef, csr_spmv, neighbors, cg_vector). */
-#define ADMP_PROFILE_KERNELS 11
+#define ADMP_PROFILE_KERNELS 12
 int admp_profile_enable(int capacity);
 int admp_profile_read(double* ms, long long* launches, double* bytes, int n);
 
@@ -272,6 +272,13 @@ typedef struct admp_pools {
   double* pos64;       /* [A,3] or NULL */
   double* box64;       /* [S,3,3] or NULL */
   void* frac64;        /* [A] double4 scratch, needed with pos64 */
+  /* optional per-slot x-key tables of QEq slots (NULL: not used): the atoms of
+   * a QEq system sorted by their first mesh plane along x (in `sorted`) and
+   * the start of each plane key, which let one thread-block cluster per
+   * system run the whole reciprocal-space matvec of a CG iteration in shared
+   * memory.  Slots whose K0 + 1 exceeds xkey_stride use the mesh passes. */
+  int* xkey;           /* [S, xkey_stride] */
+  int xkey_stride;
 } admp_pools;
 
 size_t admp_serve_slot_state_bytes(void);

@@ -68,17 +68,17 @@ __device__ __forceinline__ void make_twiddles(Cplx<T>* W, int n) {
 // ones.  Step 1 twiddles and folds the inputs (in -> out, in the butterfly's
 // own output slots), step 2 forms the output pairs (out -> in), so the result
 // of this stage is left in `in`.
-template <typename T, bool LINE_FAST>
+template <typename T, bool LINE_FAST, bool WARP>
 __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
                                              int nl, int n, int ls, int es, int Ns, int r,
-                                             const Cplx<T>* __restrict__ W, bool inverse) {
+                                             const Cplx<T>* __restrict__ W, bool inverse, int tid, int nthr) {
   const int nb = n / r;
   const int h = (r - 1) >> 1;
   const int scale = n / (Ns * r);
   const int wr = n / r;  // W[e * wr] = exp(-2 pi i e / r)
   const FastDiv f_split = fast_div(LINE_FAST ? nl : nb), f_ns = fast_div(Ns), f_items = fast_div(nl * nb);
   const int total1 = nl * nb;
-  for (int idx = threadIdx.x; idx < total1; idx += blockDim.x) {
+  for (int idx = tid; idx < total1; idx += nthr) {
     const int qd = fdiv(idx, f_split);
     const int rm = idx - qd * f_split.d;
     const int l = LINE_FAST ? rm : qd;
@@ -106,9 +106,12 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
       dst[(size_t)(base + (h + u) * Ns) * es] = dv;
     }
   }
-  __syncthreads();
+  if (WARP)
+    __syncwarp();
+  else
+    __syncthreads();
   const int total2 = (h + 1) * total1;
-  for (int idx = threadIdx.x; idx < total2; idx += blockDim.x) {
+  for (int idx = tid; idx < total2; idx += nthr) {
     const int kk = fdiv(idx, f_items);
     const int it = idx - kk * f_items.d;
     const int qd = fdiv(it, f_split);
@@ -165,13 +168,13 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
 template <typename T, bool LINE_FAST, int R>
 __device__ __forceinline__ void stockham_r35(const Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
                                              int nl, int n, int ls, int es, int Ns,
-                                             const Cplx<T>* __restrict__ W, bool inverse) {
+                                             const Cplx<T>* __restrict__ W, bool inverse, int tid, int nthr) {
   const int nb = n / R;
   const int total = nl * nb;
   const int scale = n / (Ns * R);
   const FastDiv f_split = fast_div(LINE_FAST ? nl : nb), f_ns = fast_div(Ns);
   const T sg = inverse ? T(-1) : T(1);
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+  for (int idx = tid; idx < total; idx += nthr) {
     const int qd = fdiv(idx, f_split);
     const int rm = idx - qd * f_split.d;
     const int l = LINE_FAST ? rm : qd;
@@ -236,12 +239,12 @@ __device__ __forceinline__ void stockham_r35(const Cplx<T>* __restrict__ in, Cpl
 template <typename T, bool LINE_FAST>
 __device__ __forceinline__ void stockham_r4(const Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
                                             int nl, int n, int ls, int es, int Ns,
-                                            const Cplx<T>* __restrict__ W, bool inverse) {
+                                            const Cplx<T>* __restrict__ W, bool inverse, int tid, int nthr) {
   const int nb = n >> 2;
   const int total = nl * nb;
   const int scale = n / (Ns * 4);
   const FastDiv f_split = fast_div(LINE_FAST ? nl : nb), f_ns = fast_div(Ns);
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+  for (int idx = tid; idx < total; idx += nthr) {
     const int qd = fdiv(idx, f_split);
     const int rm = idx - qd * f_split.d;
     const int l = LINE_FAST ? rm : qd;
@@ -288,12 +291,12 @@ __device__ __forceinline__ void stockham_r4(const Cplx<T>* __restrict__ in, Cplx
 template <typename T, bool LINE_FAST>
 __device__ __forceinline__ void stockham_r2(const Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
                                             int nl, int n, int ls, int es, int Ns,
-                                            const Cplx<T>* __restrict__ W, bool inverse) {
+                                            const Cplx<T>* __restrict__ W, bool inverse, int tid, int nthr) {
   const int nb = n >> 1;
   const int total = nl * nb;
   const int scale = n / (Ns * 2);
   const FastDiv f_split = fast_div(LINE_FAST ? nl : nb), f_ns = fast_div(Ns);
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+  for (int idx = tid; idx < total; idx += nthr) {
     const int qd = fdiv(idx, f_split);
     const int rm = idx - qd * f_split.d;
     const int l = LINE_FAST ? rm : qd;
@@ -318,30 +321,32 @@ __device__ __forceinline__ void stockham_r2(const Cplx<T>* __restrict__ in, Cplx
   }
 }
 
-// Full transform; returns the buffer holding the result (a or b).
-// Caller must __syncthreads() before (inputs written) -- this function
-// synchronises between stages and after the last one.
-template <typename T, bool LINE_FAST>
-__device__ Cplx<T>* fft_lines(Cplx<T>* a, Cplx<T>* b, int nl, int n, int ls, int es,
-                              const Cplx<T>* W, bool inverse) {
-  Radices R;
-  factor_radices(n, R);
+// One pass of all stages over nl lines with threads tid, tid + nthr, ...;
+// WARP: the calling threads are one warp (synchronised with __syncwarp),
+// otherwise the whole block (__syncthreads).  Returns the buffer holding the
+// result (a or b).
+template <typename T, bool LINE_FAST, bool WARP>
+__device__ __forceinline__ Cplx<T>* fft_run(const Radices& R, Cplx<T>* a, Cplx<T>* b, int nl, int n, int ls, int es,
+                                            const Cplx<T>* W, bool inverse, int tid, int nthr) {
   int Ns = 1;
   Cplx<T>* in = a;
   Cplx<T>* out = b;
   for (int s = 0; s < R.ns; ++s) {
     const int r = R.r[s];
     if (r == 4)
-      stockham_r4<T, LINE_FAST>(in, out, nl, n, ls, es, Ns, W, inverse);
+      stockham_r4<T, LINE_FAST>(in, out, nl, n, ls, es, Ns, W, inverse, tid, nthr);
     else if (r == 2)
-      stockham_r2<T, LINE_FAST>(in, out, nl, n, ls, es, Ns, W, inverse);
+      stockham_r2<T, LINE_FAST>(in, out, nl, n, ls, es, Ns, W, inverse, tid, nthr);
     else if (r == 3)
-      stockham_r35<T, LINE_FAST, 3>(in, out, nl, n, ls, es, Ns, W, inverse);
+      stockham_r35<T, LINE_FAST, 3>(in, out, nl, n, ls, es, Ns, W, inverse, tid, nthr);
     else if (r == 5)
-      stockham_r35<T, LINE_FAST, 5>(in, out, nl, n, ls, es, Ns, W, inverse);
+      stockham_r35<T, LINE_FAST, 5>(in, out, nl, n, ls, es, Ns, W, inverse, tid, nthr);
     else
-      stockham_odd<T, LINE_FAST>(in, out, nl, n, ls, es, Ns, r, W, inverse);
-    __syncthreads();
+      stockham_odd<T, LINE_FAST, WARP>(in, out, nl, n, ls, es, Ns, r, W, inverse, tid, nthr);
+    if (WARP)
+      __syncwarp();
+    else
+      __syncthreads();
     Ns *= r;
     if (r <= 5) {  // the odd-radix stage leaves its result in `in`
       Cplx<T>* tmp = in;
@@ -350,6 +355,25 @@ __device__ Cplx<T>* fft_lines(Cplx<T>* a, Cplx<T>* b, int nl, int n, int ls, int
     }
   }
   return in;
+}
+
+// Full transform by the whole block; returns the buffer holding the result (a or b).
+// Caller must __syncthreads() before (inputs written) -- this function
+// synchronises between stages and after the last one.
+template <typename T, bool LINE_FAST>
+__device__ Cplx<T>* fft_lines(Cplx<T>* a, Cplx<T>* b, int nl, int n, int ls, int es,
+                              const Cplx<T>* W, bool inverse) {
+  Radices R;
+  factor_radices(n, R);
+  return fft_run<T, LINE_FAST, false>(R, a, b, nl, n, ls, es, W, inverse, threadIdx.x, blockDim.x);
+}
+
+// One contiguous line of length n transformed by one warp (lane = 0..31),
+// ping-ponging between a and b; the caller __syncwarp()s after writing a.
+template <typename T>
+__device__ __forceinline__ Cplx<T>* warp_fft(const Radices& R, Cplx<T>* a, Cplx<T>* b, int n, const Cplx<T>* W,
+                                             bool inverse, int lane) {
+  return fft_run<T, false, true>(R, a, b, 1, n, n, 1, W, inverse, lane, 32);
 }
 
 }  // namespace admp

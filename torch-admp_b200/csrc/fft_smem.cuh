@@ -26,11 +26,14 @@ __device__ __forceinline__ void factor_radices(int n, Radices& R) {
   if (m > 1) R.r[R.ns++] = m;
 }
 
-// Division by a runtime but block-uniform divisor without the conversion /
-// reciprocal pipe: q = (x * m) >> 32 with m = ceil(2^32 / d) is exact for
-// 0 <= x < 2^16 and 1 <= d <= 2^16 (the error term x (m - 2^32/d) / 2^32 stays
-// below 1/d).  Every shared-memory index in these kernels is below 2^16 (a
-// block never holds more than 227 KB / 8 B complex values).
+// Division by a runtime but block-uniform divisor: q = (x * m) >> 32 is exact
+// for 0 <= x < 2^16 whenever 2^32/d <= m < 2^32/d + 2^16/d (the error term
+// x (m - 2^32/d) / 2^32 stays below 1/d).  On the device m comes from a
+// rounded-up single-precision reciprocal, m = floor(ru(2^32 ru(1/d))) + 1,
+// which lies in that window for 2 <= d <= 65000 (checked exhaustively over
+// every d and x); the exact integer quotient is used on the host.  Every
+// shared-memory index here is below 2^16 (a block never holds more than
+// 227 KB / 8 B complex values).
 struct FastDiv {
   int d;
   unsigned m;
@@ -38,7 +41,11 @@ struct FastDiv {
 __host__ __device__ __forceinline__ FastDiv fast_div(int d) {
   FastDiv f;
   f.d = d;
+#ifdef __CUDA_ARCH__
+  f.m = d > 1 ? (unsigned)__fmul_ru(4294967296.0f, __frcp_ru((float)d)) + 1u : 0u;
+#else
   f.m = d > 1 ? 0xFFFFFFFFu / (unsigned)d + 1u : 0u;
+#endif
   return f;
 }
 __device__ __forceinline__ int fdiv(int x, const FastDiv& f) {
@@ -56,6 +63,9 @@ __device__ __forceinline__ void make_twiddles(Cplx<T>* W, int n) {
   }
 }
 
+// Shared-memory offsets in these stages are 32-bit ints: a block never holds
+// more than 227 KB, i.e. fewer than 2^16 complex values.
+//
 // One Stockham stage with an odd prime radix r >= 7 over nl lines of length n.
 // Element (l, t) lives at buf[l * ls + t * es].  LINE_FAST selects the thread
 // mapping (consecutive threads -> consecutive lines, for layouts where the
@@ -85,13 +95,13 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
     const int j = LINE_FAST ? qd : rm;
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
-    const Cplx<T>* src = in + (size_t)l * ls;
-    Cplx<T>* dst = out + (size_t)l * ls;
+    const Cplx<T>* src = in + (int)l * ls;
+    Cplx<T>* dst = out + (int)l * ls;
     const int base = jq * Ns * r + k;
-    dst[(size_t)base * es] = src[(size_t)j * es];
+    dst[(int)base * es] = src[(int)j * es];
     for (int u = 1; u <= h; ++u) {
-      const Cplx<T> a = src[(size_t)(j + u * nb) * es];
-      const Cplx<T> c = src[(size_t)(j + (r - u) * nb) * es];
+      const Cplx<T> a = src[(int)(j + u * nb) * es];
+      const Cplx<T> c = src[(int)(j + (r - u) * nb) * es];
       const Cplx<T> wa = W[scale * k * u];
       const Cplx<T> wc = W[scale * k * (r - u)];
       const T way = inverse ? -wa.y : wa.y, wcy = inverse ? -wc.y : wc.y;
@@ -102,8 +112,8 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
       sv.y = ay + cy;
       dv.x = ax - cx;
       dv.y = ay - cy;
-      dst[(size_t)(base + u * Ns) * es] = sv;
-      dst[(size_t)(base + (h + u) * Ns) * es] = dv;
+      dst[(int)(base + u * Ns) * es] = sv;
+      dst[(int)(base + (h + u) * Ns) * es] = dv;
     }
   }
   if (WARP)
@@ -120,21 +130,21 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
     const int j = LINE_FAST ? qd : rm;
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
-    const Cplx<T>* src = out + (size_t)l * ls;
-    Cplx<T>* dst = in + (size_t)l * ls;
+    const Cplx<T>* src = out + (int)l * ls;
+    Cplx<T>* dst = in + (int)l * ls;
     const int base = jq * Ns * r + k;
-    const Cplx<T> v0 = src[(size_t)base * es];
+    const Cplx<T> v0 = src[(int)base * es];
     T ax = v0.x, ay = v0.y;
     if (kk == 0) {
       for (int u = 1; u <= h; ++u) {
-        const Cplx<T> sv = src[(size_t)(base + u * Ns) * es];
+        const Cplx<T> sv = src[(int)(base + u * Ns) * es];
         ax += sv.x;
         ay += sv.y;
       }
       Cplx<T> X;
       X.x = ax;
       X.y = ay;
-      dst[(size_t)base * es] = X;
+      dst[(int)base * es] = X;
       continue;
     }
     T bx = 0, by = 0;
@@ -143,8 +153,8 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
       e += kk;
       if (e >= r) e -= r;
       const Cplx<T> w = W[e * wr];  // (cos, -sin) of 2 pi e / r
-      const Cplx<T> sv = src[(size_t)(base + u * Ns) * es];
-      const Cplx<T> dv = src[(size_t)(base + (h + u) * Ns) * es];
+      const Cplx<T> sv = src[(int)(base + u * Ns) * es];
+      const Cplx<T> dv = src[(int)(base + (h + u) * Ns) * es];
       ax += sv.x * w.x;
       ay += sv.y * w.x;
       bx -= dv.x * w.y;
@@ -157,8 +167,8 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
     X1.y = ay + iby;
     X2.x = ax - ibx;
     X2.y = ay - iby;
-    dst[(size_t)(base + kk * Ns) * es] = X1;
-    dst[(size_t)(base + (r - kk) * Ns) * es] = X2;
+    dst[(int)(base + kk * Ns) * es] = X1;
+    dst[(int)(base + (r - kk) * Ns) * es] = X2;
   }
 }
 
@@ -181,11 +191,11 @@ __device__ __forceinline__ void stockham_r35(const Cplx<T>* __restrict__ in, Cpl
     const int j = LINE_FAST ? qd : rm;
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
-    const Cplx<T>* src = in + (size_t)l * ls;
+    const Cplx<T>* src = in + (int)l * ls;
     Cplx<T> v[R];
 #pragma unroll
     for (int t = 0; t < R; ++t) {
-      const Cplx<T> x = src[(size_t)(j + t * nb) * es];
+      const Cplx<T> x = src[(int)(j + t * nb) * es];
       if (t == 0) {
         v[0] = x;
       } else {
@@ -229,9 +239,9 @@ __device__ __forceinline__ void stockham_r35(const Cplx<T>* __restrict__ in, Cpl
       X[3].y = p2y + q2x;
     }
     const int base = jq * Ns * R + k;
-    Cplx<T>* dst = out + (size_t)l * ls;
+    Cplx<T>* dst = out + (int)l * ls;
 #pragma unroll
-    for (int u = 0; u < R; ++u) dst[(size_t)(base + u * Ns) * es] = X[u];
+    for (int u = 0; u < R; ++u) dst[(int)(base + u * Ns) * es] = X[u];
   }
 }
 
@@ -251,11 +261,11 @@ __device__ __forceinline__ void stockham_r4(const Cplx<T>* __restrict__ in, Cplx
     const int j = LINE_FAST ? qd : rm;
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
-    const Cplx<T>* src = in + (size_t)l * ls;
+    const Cplx<T>* src = in + (int)l * ls;
     Cplx<T> v[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-      Cplx<T> x = src[(size_t)(j + t * nb) * es];
+      Cplx<T> x = src[(int)(j + t * nb) * es];
       if (t == 0) {
         v[0] = x;
       } else {
@@ -274,16 +284,16 @@ __device__ __forceinline__ void stockham_r4(const Cplx<T>* __restrict__ in, Cplx
     T mdx = inverse ? -dy : dy;
     T mdy = inverse ? dx : -dx;
     const int base = jq * Ns * 4 + k;
-    Cplx<T>* dst = out + (size_t)l * ls;
+    Cplx<T>* dst = out + (int)l * ls;
     Cplx<T> o0, o1, o2, o3;
     o0.x = ax + cx; o0.y = ay + cy;
     o1.x = bx + mdx; o1.y = by + mdy;
     o2.x = ax - cx; o2.y = ay - cy;
     o3.x = bx - mdx; o3.y = by - mdy;
-    dst[(size_t)(base) * es] = o0;
-    dst[(size_t)(base + Ns) * es] = o1;
-    dst[(size_t)(base + 2 * Ns) * es] = o2;
-    dst[(size_t)(base + 3 * Ns) * es] = o3;
+    dst[(int)(base) * es] = o0;
+    dst[(int)(base + Ns) * es] = o1;
+    dst[(int)(base + 2 * Ns) * es] = o2;
+    dst[(int)(base + 3 * Ns) * es] = o3;
   }
 }
 
@@ -303,21 +313,21 @@ __device__ __forceinline__ void stockham_r2(const Cplx<T>* __restrict__ in, Cplx
     const int j = LINE_FAST ? qd : rm;
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
-    const Cplx<T>* src = in + (size_t)l * ls;
-    Cplx<T> a = src[(size_t)j * es];
-    Cplx<T> x = src[(size_t)(j + nb) * es];
+    const Cplx<T>* src = in + (int)l * ls;
+    Cplx<T> a = src[(int)j * es];
+    Cplx<T> x = src[(int)(j + nb) * es];
     Cplx<T> w = W[scale * k];
     T wy = inverse ? -w.y : w.y;
     Cplx<T> b;
     b.x = x.x * w.x - x.y * wy;
     b.y = x.x * wy + x.y * w.x;
     const int base = jq * Ns * 2 + k;
-    Cplx<T>* dst = out + (size_t)l * ls;
+    Cplx<T>* dst = out + (int)l * ls;
     Cplx<T> o0, o1;
     o0.x = a.x + b.x; o0.y = a.y + b.y;
     o1.x = a.x - b.x; o1.y = a.y - b.y;
-    dst[(size_t)base * es] = o0;
-    dst[(size_t)(base + Ns) * es] = o1;
+    dst[(int)base * es] = o0;
+    dst[(int)(base + Ns) * es] = o1;
   }
 }
 

@@ -57,13 +57,13 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   lp = lp < 1 ? 1 : (lp > 64 ? 64 : lp);
   while (lp > 1 && (2 * (size_t)lp + 1) * maxK[2] * cs > budget) --lp;
   b.lp = lp;
-  int zb = sizeof(T) == 4 ? 16 : 8;
+  int zb = sizeof(T) == 4 ? 32 : 16;
   const int mk01 = maxK[0] > maxK[1] ? maxK[0] : maxK[1];
-  while (zb > 1 && (2 * (size_t)zb + 1) * mk01 * cs + (mk01 + zb) * 8 > budget) zb >>= 1;
+  while (zb > 1 && (2 * (size_t)zb + 1) * mk01 * cs + (mk01 + 2 * zb) * 8 + zb * 16 > budget) zb >>= 1;
   b.zb = zb;
   p.smem_z = (2 * (size_t)lp + 1) * maxK[2] * cs;
   p.smem_y = (2 * (size_t)zb + 1) * maxK[1] * cs;
-  p.smem_x = (2 * (size_t)zb + 1) * maxK[0] * cs + ((size_t)maxK[0] + zb) * 8;
+  p.smem_x = (2 * (size_t)zb + 1) * maxK[0] * cs + ((size_t)maxK[0] + 2 * zb) * 8 + (size_t)zb * 16;
   if (p.smem_z > 227 * 1024 || p.smem_y > 227 * 1024 || p.smem_x > 227 * 1024)
     return fail(ADMP_ERR_MESH, "mesh %dx%dx%d too large for the shared-memory FFT", maxK[0], maxK[1], maxK[2]);
   int ba = 0, bz = 0, by = 0, bx = 0;
@@ -90,7 +90,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
     ba += (d.natoms + b.apb - 1) / b.apb;
     bz += ((d.K0 * d.K1 + 1) / 2 + lp - 1) / lp;
     by += d.K0 * ncb;
-    bx += d.K1 * ncb;
+    bx += (d.K1 * d.K2h + zb - 1) / zb;  // x passes: runs of zb flattened (y, kz) columns
     mo += align_up((size_t)d.K0 * d.K1 * d.K2, 64);
     so += align_up((size_t)d.K0 * d.K1 * d.K2h, 32);
   }

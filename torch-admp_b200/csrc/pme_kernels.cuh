@@ -341,21 +341,32 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h, zb = b.zb;
-  const int ncb = (K2h + zb - 1) / zb;
-  const int local = blockIdx.x - d.blk_x;
-  const int y = local / ncb, cb = local - y * ncb;
-  const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  // this block: columns [c0, c0 + nz) of the flattened (y, kz) index c = y K2h + kz
+  const int c0 = (blockIdx.x - d.blk_x) * zb, nz = min(zb, K1 * K2h - c0);
   const FastDiv fdnz = fast_div(nz);
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
   Cplx<T>* A = W + b.maxK0;
   Cplx<T>* B = A + (size_t)zb * b.maxK0;
   double* thx = reinterpret_cast<double*>(B + (size_t)zb * b.maxK0);
-  double* thz = thx + b.maxK0;
+  double* thyz = thx + b.maxK0;   // theta_y theta_z per column
+  double* wcol = thyz + zb;       // half-spectrum weight per column
+  int* lab = reinterpret_cast<int*>(wcol + zb);  // per column: ny, mirror ny, nz, mirror nz
   make_twiddles(W, K0);
   load_geom(box, d.box_idx, &g);
   for (int i = threadIdx.x; i < K0; i += blockDim.x) thx[i] = theta_1d(signed_k(i, K0), K0);
-  for (int i = threadIdx.x; i < nz; i += blockDim.x) thz[i] = theta_1d(signed_k(kz0 + i, K2), K2);
-  Cplx<T>* H = spec + d.spec_off + (size_t)y * K2h + kz0;
+  for (int i = threadIdx.x; i < nz; i += blockDim.x) {
+    const int c = c0 + i, y = c / K2h, kz = c - y * K2h;
+    // labels of the mirror indices -y, -kz (the reference labels K/2 as -K/2,
+    // so a Nyquist index is its own mirror with the same label)
+    const int ny = signed_k(y, K1), n2 = signed_k(kz, K2);
+    lab[4 * i] = ny;
+    lab[4 * i + 1] = signed_k(y == 0 ? 0 : K1 - y, K1);
+    lab[4 * i + 2] = n2;
+    lab[4 * i + 3] = signed_k(kz == 0 ? 0 : K2 - kz, K2);
+    thyz[i] = theta_1d(ny, K1) * theta_1d(n2, K2);
+    wcol[i] = (kz == 0 || (2 * kz == K2)) ? 1.0 : 2.0;
+  }
+  Cplx<T>* H = spec + d.spec_off + c0;
   const size_t xs = (size_t)K1 * K2h;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
     const int x = fdiv(idx, fdnz), c = idx - x * nz;
@@ -366,28 +377,22 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
   Cplx<T>* F = (R == A) ? B : A;
   const double kappa = d.kappa;
   const double inv4k2 = 1.0 / (4.0 * kappa * kappa);
-  const int ny = signed_k(y, K1);
-  // label of the mirror index -y mod K1 (the reference labels K/2 as -K/2, so a
-  // Nyquist index is its own mirror with the same label)
-  const int nyb = signed_k(y == 0 ? 0 : K1 - y, K1);
-  const double thy = theta_1d(ny, K1);
   const double pref = ke * 2.0 * kPi / g.vol;
   double v[10];
 #pragma unroll
   for (int k = 0; k < 10; ++k) v[k] = 0.0;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
     const int x = fdiv(idx, fdnz), c = idx - x * nz;
-    const int kz = kz0 + c;
     // A half-spectrum entry p stands for p and its mirror pb = -p (mod K); both
     // carry |S|^2 and the reference's own integer labels.  E = sum G(n)|S|^2
     // over the full spectrum equals sum over the half spectrum of
     // w * Gs * |S|^2 with Gs = (G(n_p) + G(n_pb)) / 2 and w = 2 (1 on the
     // kz = 0 and kz = K2/2 planes, whose mirrors are separate entries).
-    const int n0 = signed_k(x, K0), n2 = signed_k(kz, K2);
-    const int n0b = signed_k(x == 0 ? 0 : K0 - x, K0), n2b = signed_k(kz == 0 ? 0 : K2 - kz, K2);
-    const double th = thx[x] * thy * thz[c];
+    const int ny = lab[4 * c], nyb = lab[4 * c + 1], n2 = lab[4 * c + 2], n2b = lab[4 * c + 3];
+    const int n0 = signed_k(x, K0), n0b = signed_k(x == 0 ? 0 : K0 - x, K0);
+    const double th = thx[x] * thyz[c];
     const double inv_th2 = 1.0 / (th * th);
-    const double w = (kz == 0 || (2 * kz == K2)) ? 1.0 : 2.0;
+    const double w = wcol[c];
     Cplx<T> S = R[x * zb + c];
     const double s2 = (double)S.x * (double)S.x + (double)S.y * (double)S.y;
     double Gs = 0.0;
@@ -549,23 +554,20 @@ __global__ void __launch_bounds__(256) green_build_kernel(Batch b, const T* __re
   const int s = find_sys<F_X>(b, blockIdx.x);
   const SysDesc& d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h, zb = b.zb;
-  const int ncb = (K2h + zb - 1) / zb;
-  const int local = blockIdx.x - d.blk_x;
-  const int y = local / ncb, cb = local - y * ncb;
-  const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  const int c0 = (blockIdx.x - d.blk_x) * zb, nz = min(zb, K1 * K2h - c0);
   const FastDiv fdnz = fast_div(nz);
   load_geom(box, d.box_idx, &g);
   __syncthreads();
   const double inv4k2 = 1.0 / (4.0 * d.kappa * d.kappa);
   const double pref = ke * 2.0 * kPi / g.vol;
-  const int ny = signed_k(y, K1), nyb = signed_k(y == 0 ? 0 : K1 - y, K1);
-  const double thy = theta_1d(ny, K1);
-  T* G = green + d.green_off + (size_t)y * K2h + kz0;
+  T* G = green + d.green_off + c0;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = fdiv(idx, fdnz), c = idx - x * nz, kz = kz0 + c;
+    const int x = fdiv(idx, fdnz), c = idx - x * nz;
+    const int cc = c0 + c, y = cc / K2h, kz = cc - y * K2h;
+    const int ny = signed_k(y, K1), nyb = signed_k(y == 0 ? 0 : K1 - y, K1);
     const int n0 = signed_k(x, K0), n2 = signed_k(kz, K2);
     const int n0b = signed_k(x == 0 ? 0 : K0 - x, K0), n2b = signed_k(kz == 0 ? 0 : K2 - kz, K2);
-    const double th = theta_1d(n0, K0) * thy * theta_1d(n2, K2);
+    const double th = theta_1d(n0, K0) * theta_1d(ny, K1) * theta_1d(n2, K2);
     const bool same = (n0b == -n0) && (nyb == -ny) && (n2b == -n2);
     double Gs = 0.0;
     for (int m = 0; m < 2; ++m) {
@@ -590,17 +592,15 @@ __global__ void __launch_bounds__(256) fft_x_apply_kernel(Batch b, Cplx<T>* __re
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2h = d.K2h, zb = b.zb;
-  const int ncb = (K2h + zb - 1) / zb;
-  const int local = blockIdx.x - d.blk_x;
-  const int y = local / ncb, cb = local - y * ncb;
-  const int kz0 = cb * zb, nz = min(zb, K2h - kz0);
+  // this block: columns [c0, c0 + nz) of the flattened (y, kz) index c = y K2h + kz
+  const int c0 = (blockIdx.x - d.blk_x) * zb, nz = min(zb, K1 * K2h - c0);
   const FastDiv fdnz = fast_div(nz);
   Cplx<T>* W = reinterpret_cast<Cplx<T>*>(smem_raw);
   Cplx<T>* A = W + b.maxK0;
   Cplx<T>* B = A + (size_t)zb * b.maxK0;
   make_twiddles(W, K0);
-  Cplx<T>* H = spec + d.spec_off + (size_t)y * K2h + kz0;
-  const T* G = green + d.green_off + (size_t)y * K2h + kz0;
+  Cplx<T>* H = spec + d.spec_off + c0;
+  const T* G = green + d.green_off + c0;
   const size_t xs = (size_t)K1 * K2h;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
     const int x = fdiv(idx, fdnz), c = idx - x * nz;

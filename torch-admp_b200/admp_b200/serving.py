@@ -240,6 +240,12 @@ class ServingEngine:
         self._fact_cache: Dict[int, tuple] = {}
         self._inflight: List[tuple] = []  # launched work whose results are not read yet, in launch order
         self._zeros = {dt: torch.zeros(3 * 64, dtype=dt, device=self.dev) for dt in (torch.float32, torch.float64)}
+        # upload scratch: box rows of one admission on the device, pinned host staging (ring of three)
+        self._box_stage = {dt: torch.zeros(max_slots, 9, dtype=dt, device=self.dev)
+                           for dt in (torch.float32, torch.float64)}
+        self._stage_ring = [[None, None, []] for _ in range(3)]
+        self._stage_k = 0
+        self._stage_off = 0
         # host seconds per scheduler phase (admission + upload, launches, waiting on the device, reading results)
         self.host_time = {"admit": 0.0, "launch": 0.0, "wait": 0.0, "results": 0.0}
         # results as host numpy arrays (True) or device tensors (False)
@@ -389,30 +395,68 @@ class ServingEngine:
             runs.append(cur)
         return runs
 
-    def _stack(self, arrays, dtype, pads=None, width=1):
-        """Concatenate request arrays into one source tensor, with pads[k] zero
-        rows (of `width` values) after array k: device tensors with one
-        torch.cat, host arrays through one pinned buffer.  Returns
-        (tensor, host bytes)."""
+    def _stage_begin(self) -> None:
+        """Start an upload on the next of three pinned host staging buffers; a
+        buffer is reused only after the copies of its previous upload ran."""
+        self._stage_k = (self._stage_k + 1) % 3
+        buf, ev, _ = self._stage_ring[self._stage_k]
+        if ev is not None:
+            ev.synchronize()
+        self._stage_ring[self._stage_k] = [buf, None, []]
+        self._stage_off = 0
+
+    def _stage_end(self) -> None:
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        self._stage_ring[self._stage_k][1] = ev
+
+    def _stage_take(self, n: int, npdt) -> np.ndarray:
+        """n values of numpy dtype npdt from the current staging buffer (grown,
+        keeping the old one alive until this upload's copies ran, if too small)."""
+        slot = self._stage_ring[self._stage_k]
+        item = np.dtype(npdt).itemsize
+        off = (self._stage_off + 63) // 64 * 64
+        need = off + n * item
+        if slot[0] is None or slot[0].numel() < need:
+            if slot[0] is not None:
+                slot[2].append(slot[0])
+            cap = max(need, 2 * (slot[0].numel() if slot[0] is not None else 0), 1 << 24)
+            slot[0] = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
+            off, need = 0, n * item
+        self._stage_off = need
+        return slot[0][off:need].numpy().view(npdt), slot[0][off:need].view(
+            {np.float32: torch.float32, np.float64: torch.float64}[npdt])
+
+    def _fill(self, dest, arrays, pads=None, width=1) -> int:
+        """Write the request arrays, with pads[k] zero rows (of `width` values)
+        after array k, into the contiguous pool slice `dest` without allocating:
+        device tensors with one torch.cat into `dest`, host arrays through the
+        pinned staging buffer and one copy.  Returns the host bytes copied."""
         pads = pads or [0] * len(arrays)
+        dtype = dest.dtype
         if isinstance(arrays[0], torch.Tensor):
-            # rows of `width` values, concatenated along dim 0 (one batched copy)
             parts = []
             zero = self._zeros[dtype]
             for a, p in zip(arrays, pads):
-                parts.append(a if a.dtype == dtype else a.to(dtype))
+                a = a if a.dtype == dtype else a.to(dtype)
+                parts.append(a.reshape(-1, width) if width > 1 else a.reshape(-1))
                 if p:
-                    parts.append(zero[:p * width].view(p, width) if a.dim() == 2 else zero[:p * width])
-            return (torch.cat(parts) if len(parts) > 1 else parts[0]).reshape(-1), 0
+                    parts.append(zero[:p * width].view(p, width) if width > 1 else zero[:p])
+            torch.cat(parts, out=dest.view(-1, width) if width > 1 else dest.view(-1))
+            return 0
         npdt = {torch.float32: np.float32, torch.float64: np.float64}[dtype]
-        parts = []
+        n = dest.numel()
+        host, th = self._stage_take(n, npdt)
+        o = 0
         for a, p in zip(arrays, pads):
-            parts.append(np.asarray(a, dtype=npdt).reshape(-1))
+            v = np.asarray(a).reshape(-1)
+            host[o:o + v.size] = v
+            o += v.size
             if p:
-                parts.append(np.zeros(p * width, dtype=npdt))
-        host = np.concatenate(parts) if len(parts) > 1 else parts[0]
-        t = torch.from_numpy(host).pin_memory()
-        return t, t.numel() * t.element_size()
+                host[o:o + p * width] = 0
+                o += p * width
+        dest.view(-1).copy_(th, non_blocking=True)
+        return n * th.element_size()
 
     @staticmethod
     def _pads(run):
@@ -423,26 +467,28 @@ class ServingEngine:
         t = self.t
         nb = 0
         has64 = "pos64" in t
+        self._stage_begin()
+        n = len(items)
         slots = torch.tensor([a.slot for a in items], dtype=torch.long).to(self.dev, non_blocking=True)
-        boxes, b = self._stack([a.req.box for a in items], torch.float64 if has64 else self.dtype)
-        nb += b
-        boxes = boxes.to(self.dev, non_blocking=True).reshape(-1, 3, 3)
+        bdt = torch.float64 if has64 else self.dtype
+        boxes = self._box_stage[bdt][:n]
+        nb += self._fill(boxes, [a.req.box for a in items], width=9)
         if has64:
-            t["box64"].index_copy_(0, slots, boxes)
-        t["box"].index_copy_(0, slots, boxes.to(self.dtype))
+            t["box64"].index_copy_(0, slots, boxes.view(-1, 3, 3))
+            t["box"].index_copy_(0, slots, boxes.view(-1, 3, 3).to(self.dtype))
+        else:
+            t["box"].index_copy_(0, slots, boxes.view(-1, 3, 3))
         for run in self._runs(items):
             lo = run[0].atom_off
             hi = run[-1].atom_off + run[-1].req.natoms
             sl = slice(lo, hi)
             pads = self._pads(run)
-            pos, b = self._stack([a.req.pos for a in run], torch.float64 if has64 else self.dtype, pads, 3)
-            nb += b
             if has64:
                 # positions arrive in double; the FP32 copy is made on the device
-                t["pos64"][sl].copy_(pos.reshape(-1, 3), non_blocking=True)
+                nb += self._fill(t["pos64"][sl], [a.req.pos for a in run], pads, 3)
                 t["pos"][sl].copy_(t["pos64"][sl], non_blocking=True)
             else:
-                t["pos"][sl].copy_(pos.reshape(-1, 3), non_blocking=True)
+                nb += self._fill(t["pos"][sl], [a.req.pos for a in run], pads, 3)
             # runs of one kind (PME first, then QEq, within a tick)
             k = 0
             while k < len(run):
@@ -453,14 +499,10 @@ class ServingEngine:
                 ssl = slice(sub[0].atom_off, sub[-1].atom_off + sub[-1].req.natoms)
                 spads = pads[k:j - 1] + [0]
                 if sub[0].kind == SYS_PME:
-                    q, b = self._stack([a.req.charges for a in sub], self.dtype, spads)
-                    t["q"][ssl].copy_(q, non_blocking=True)
-                    nb += b
+                    nb += self._fill(t["q"][ssl], [a.req.charges for a in sub], spads)
                 else:
                     for name in ("chi", "hardness", "eta"):
-                        v, b = self._stack([getattr(a.req, name) for a in sub], self.dtype, spads)
-                        t[name][ssl].copy_(v, non_blocking=True)
-                        nb += b
+                        nb += self._fill(t[name][ssl], [getattr(a.req, name) for a in sub], spads)
                     t["q"][ssl].zero_()
                     for a in sub:
                         key = a.req.meta.get("system_id") if a.req.meta else None
@@ -470,6 +512,7 @@ class ServingEngine:
                                 np.asarray(w, dtype=np.float32 if self.dtype == torch.float32 else np.float64))
                             t["q"][a.atom_off:a.atom_off + a.req.natoms].copy_(src, non_blocking=True)
                 k = j
+        self._stage_end()
         self.stats["h2d_bytes"] += nb
 
     def _launch_finish(self, items: List[_Active]):

@@ -100,13 +100,13 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   b.nblk_x = bx;
   p.mesh_elems = mo;
   p.spec_elems = so;
-  // fused slab passes: buffers of max(ceil(K1/2) K2, K1 (K2/2+1)) complex, two of them, plus twiddles
-  int be = 0;
+  // fused slab passes: two buffers of at least one plane (max(ceil(K1/2) K2, K1 (K2/2+1)) complex) and at
+  // least kSlabTarget complex values, so that small meshes take several planes per block; plus twiddles
+  const int kSlabTarget = sizeof(T) == 4 ? 3072 : 1536;
+  int be = kSlabTarget;
   for (int s = 0; s < nsys; ++s) {
-    const int a = ((sys[s].K[1] + 1) / 2) * sys[s].K[2];
-    const int c = sys[s].K[1] * (sys[s].K[2] / 2 + 1);
+    const int a = slab_plane_elems(sys[s].K[1], sys[s].K[2]);
     be = be > a ? be : a;
-    be = be > c ? be : c;
   }
   p.buf_elems = be;
   p.smem_slab = (2 * (size_t)be + maxK[1] + maxK[2]) * cs;
@@ -114,7 +114,8 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   p.nblk_slab = 0;
   for (int s = 0; s < nsys; ++s) {
     p.blk_slab[s] = p.nblk_slab;
-    p.nblk_slab += sys[s].K[0];
+    const int ppb = slab_ppb(be, slab_plane_elems(sys[s].K[1], sys[s].K[2]), sys[s].K[0]);
+    p.nblk_slab += (sys[s].K[0] + ppb - 1) / ppb;
   }
   return ADMP_OK;
 }

@@ -436,56 +436,85 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
 }
 
 // ---------------------------------------------------------------------------
-// Fused slab passes (one block per x plane, when a plane fits in shared memory):
+// Fused slab passes (a block takes ppb consecutive x planes when they fit in
+// shared memory; small meshes get several planes per block so every FFT
+// stage has enough lines for the whole block):
 //   fft_slab_fwd: Q[x][y][z] -> z R2C (two real lines per complex FFT) -> y FFT
 //                 -> H[x][y][kz]
 //   fft_slab_inv: H[x][y][kz] -> inverse y FFT -> z C2R -> phi[x][y][z]
+// In shared memory the z lines of the block's planes are packed back to back
+// (line (pl, p) at (pl np + p) K2) and the y lines interleaved by plane
+// (element (y, pl, kz) at (y npl + pl) K2h + kz), so each pass is one batch
+// of equally strided lines.
 // ---------------------------------------------------------------------------
+// planes per block for a system whose plane needs PL complex values, given
+// the launch's per-buffer capacity (the host computes block counts the same way)
+__host__ __device__ inline int slab_ppb(int buf_elems, int PL, int K0) {
+  int p = buf_elems / PL;
+  p = p < 1 ? 1 : p;
+  return p < K0 ? p : K0;
+}
+
+__host__ __device__ inline int slab_plane_elems(int K1, int K2) {
+  const int a = ((K1 + 1) / 2) * K2, c = K1 * (K2 / 2 + 1);
+  return a > c ? a : c;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __restrict__ mesh,
                                                            Cplx<T>* __restrict__ spec, int buf_elems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int s = find_sys<F_Y>(b, blockIdx.x);  // F_Y blocks are remapped to one per x plane
+  const int s = find_sys<F_Y>(b, blockIdx.x);  // F_Y blocks are remapped to runs of x planes
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
-  const int K1 = d.K1, K2 = d.K2, K2h = d.K2h;
-  const FastDiv fdK2 = fast_div(K2), fdK2h = fast_div(K2h);
-  const int x = blockIdx.x - d.blk_y;
+  const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h;
   const int np = (K1 + 1) / 2;
+  const int ppb = slab_ppb(buf_elems, slab_plane_elems(K1, K2), K0);
+  const int x0 = (blockIdx.x - d.blk_y) * ppb, npl = min(ppb, K0 - x0);
+  const FastDiv fdK2 = fast_div(K2), fdK2h = fast_div(K2h), fdnp = fast_div(np), fdP = fast_div(K1 * K2h);
   Cplx<T>* W1 = reinterpret_cast<Cplx<T>*>(smem_raw);
   Cplx<T>* W2 = W1 + b.maxK1;
   Cplx<T>* A = W2 + b.maxK2;
   Cplx<T>* B = A + buf_elems;
   make_twiddles(W1, K1);
   make_twiddles(W2, K2);
-  const T* Q = mesh + d.mesh_off + (size_t)x * K1 * K2;
-  for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
-    const int p = fdiv(idx, fdK2), t = idx - p * K2;
+  const T* Q = mesh + d.mesh_off + (size_t)x0 * K1 * K2;
+  const int nzl = npl * np;  // z line pairs of the block
+  for (int idx = threadIdx.x; idx < nzl * K2; idx += blockDim.x) {
+    const int line = fdiv(idx, fdK2), t = idx - line * K2;
+    const int pl = fdiv(line, fdnp), p = line - pl * np;
+    const T* Qp = Q + (size_t)pl * K1 * K2;
     Cplx<T> z;
-    z.x = Q[(size_t)(2 * p) * K2 + t];
-    z.y = 2 * p + 1 < K1 ? Q[(size_t)(2 * p + 1) * K2 + t] : T(0);
-    A[p * K2 + t] = z;
+    z.x = Qp[(size_t)(2 * p) * K2 + t];
+    z.y = 2 * p + 1 < K1 ? Qp[(size_t)(2 * p + 1) * K2 + t] : T(0);
+    A[idx] = z;
   }
   __syncthreads();
-  Cplx<T>* R = fft_lines<T, false>(A, B, np, K2, K2, 1, W2, false);
+  Cplx<T>* R = fft_lines<T, false>(A, B, nzl, K2, K2, 1, W2, false);
   Cplx<T>* U = (R == A) ? B : A;
-  // unpack the two-for-one transforms into U[y][kz]
-  for (int idx = threadIdx.x; idx < np * K2h; idx += blockDim.x) {
-    const int p = fdiv(idx, fdK2h), k = idx - p * K2h;
-    const Cplx<T> Z = R[p * K2 + k];
-    const Cplx<T> Zm = R[p * K2 + (k == 0 ? 0 : K2 - k)];
+  // unpack the two-for-one transforms into U[y][pl][kz]
+  const int ys = npl * K2h;  // element stride of the y lines
+  for (int idx = threadIdx.x; idx < nzl * K2h; idx += blockDim.x) {
+    const int line = fdiv(idx, fdK2h), k = idx - line * K2h;
+    const int pl = fdiv(line, fdnp), p = line - pl * np;
+    const Cplx<T> Z = R[line * K2 + k];
+    const Cplx<T> Zm = R[line * K2 + (k == 0 ? 0 : K2 - k)];
     Cplx<T> a, c;
     a.x = (Z.x + Zm.x) * T(0.5);
     a.y = (Z.y - Zm.y) * T(0.5);
     c.x = (Z.y + Zm.y) * T(0.5);
     c.y = (Zm.x - Z.x) * T(0.5);
-    U[(2 * p) * K2h + k] = a;
-    if (2 * p + 1 < K1) U[(2 * p + 1) * K2h + k] = c;
+    U[(2 * p) * ys + pl * K2h + k] = a;
+    if (2 * p + 1 < K1) U[(2 * p + 1) * ys + pl * K2h + k] = c;
   }
   __syncthreads();
-  Cplx<T>* V = fft_lines<T, true>(U, R, K2h, K1, 1, K2h, W1, false);
-  Cplx<T>* H = spec + d.spec_off + (size_t)x * K1 * K2h;
-  for (int idx = threadIdx.x; idx < K1 * K2h; idx += blockDim.x) H[idx] = V[idx];
+  Cplx<T>* V = fft_lines<T, true>(U, R, npl * K2h, K1, 1, ys, W1, false);
+  Cplx<T>* H = spec + d.spec_off + (size_t)x0 * K1 * K2h;
+  for (int idx = threadIdx.x; idx < npl * K1 * K2h; idx += blockDim.x) {
+    const int pl = fdiv(idx, fdP), rem = idx - pl * (K1 * K2h);
+    const int y = fdiv(rem, fdK2h), kz = rem - y * K2h;
+    H[idx] = V[y * ys + pl * K2h + kz];
+  }
 }
 
 template <typename T>
@@ -495,29 +524,37 @@ __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T
   const int s = find_sys<F_Y>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
-  const int K1 = d.K1, K2 = d.K2, K2h = d.K2h;
-  const FastDiv fdK2 = fast_div(K2);
-  const int x = blockIdx.x - d.blk_y;
+  const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h;
   const int np = (K1 + 1) / 2;
+  const int ppb = slab_ppb(buf_elems, slab_plane_elems(K1, K2), K0);
+  const int x0 = (blockIdx.x - d.blk_y) * ppb, npl = min(ppb, K0 - x0);
+  const FastDiv fdK2 = fast_div(K2), fdK2h = fast_div(K2h), fdnp = fast_div(np), fdP = fast_div(K1 * K2h);
   Cplx<T>* W1 = reinterpret_cast<Cplx<T>*>(smem_raw);
   Cplx<T>* W2 = W1 + b.maxK1;
   Cplx<T>* A = W2 + b.maxK2;
   Cplx<T>* B = A + buf_elems;
   make_twiddles(W1, K1);
   make_twiddles(W2, K2);
-  const Cplx<T>* H = spec + d.spec_off + (size_t)x * K1 * K2h;
-  for (int idx = threadIdx.x; idx < K1 * K2h; idx += blockDim.x) A[idx] = H[idx];
+  const int ys = npl * K2h;
+  const Cplx<T>* H = spec + d.spec_off + (size_t)x0 * K1 * K2h;
+  for (int idx = threadIdx.x; idx < npl * K1 * K2h; idx += blockDim.x) {
+    const int pl = fdiv(idx, fdP), rem = idx - pl * (K1 * K2h);
+    const int y = fdiv(rem, fdK2h), kz = rem - y * K2h;
+    A[y * ys + pl * K2h + kz] = H[idx];
+  }
   __syncthreads();
-  Cplx<T>* V = fft_lines<T, true>(A, B, K2h, K1, 1, K2h, W1, true);
+  Cplx<T>* V = fft_lines<T, true>(A, B, npl * K2h, K1, 1, ys, W1, true);
   Cplx<T>* Z = (V == A) ? B : A;
-  for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
-    const int p = fdiv(idx, fdK2), t = idx - p * K2;
+  const int nzl = npl * np;
+  for (int idx = threadIdx.x; idx < nzl * K2; idx += blockDim.x) {
+    const int line = fdiv(idx, fdK2), t = idx - line * K2;
+    const int pl = fdiv(line, fdnp), p = line - pl * np;
     const bool lo = t < K2h;
     const int tt = lo ? t : K2 - t;
-    Cplx<T> a = V[(2 * p) * K2h + tt];
+    Cplx<T> a = V[(2 * p) * ys + pl * K2h + tt];
     Cplx<T> c;
     if (2 * p + 1 < K1) {
-      c = V[(2 * p + 1) * K2h + tt];
+      c = V[(2 * p + 1) * ys + pl * K2h + tt];
     } else {
       c.x = T(0);
       c.y = T(0);
@@ -529,16 +566,18 @@ __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T
     Cplx<T> z;
     z.x = a.x - c.y;
     z.y = a.y + c.x;
-    Z[p * K2 + t] = z;
+    Z[idx] = z;
   }
   __syncthreads();
-  Cplx<T>* R = fft_lines<T, false>(Z, V, np, K2, K2, 1, W2, true);
-  T* M = mesh + d.mesh_off + (size_t)x * K1 * K2;
-  for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
-    const int p = fdiv(idx, fdK2), t = idx - p * K2;
-    const Cplx<T> z = R[p * K2 + t];
-    M[(size_t)(2 * p) * K2 + t] = z.x;
-    if (2 * p + 1 < K1) M[(size_t)(2 * p + 1) * K2 + t] = z.y;
+  Cplx<T>* R = fft_lines<T, false>(Z, V, nzl, K2, K2, 1, W2, true);
+  T* M = mesh + d.mesh_off + (size_t)x0 * K1 * K2;
+  for (int idx = threadIdx.x; idx < nzl * K2; idx += blockDim.x) {
+    const int line = fdiv(idx, fdK2), t = idx - line * K2;
+    const int pl = fdiv(line, fdnp), p = line - pl * np;
+    const Cplx<T> z = R[idx];
+    T* Mp = M + (size_t)pl * K1 * K2;
+    Mp[(size_t)(2 * p) * K2 + t] = z.x;
+    if (2 * p + 1 < K1) Mp[(size_t)(2 * p + 1) * K2 + t] = z.y;
   }
 }
 

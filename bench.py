@@ -49,6 +49,10 @@ RCUT, ETHRESH = 6.0, 5e-4
 # force error ~2e-4)
 TOL = 1e-7
 LAT_RATE = 1000.0      # open-loop Poisson rate (requests/s) for the p50/p99 latency pass
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte, from one ncu capture of
+# the 400-request stream (x_apply 83.4 MB per launch, spread 58.4, gather 63.9); roofline.traffic = ratio x algorithmic bytes
+# per launch of this run, the launches of one chunk being alike in size at 400 and 2000 requests
+TRAFFIC_PER_ALG_BYTE = {"fft_x_green": 0.796, "spread": 1.216, "gather": 1.280}
 
 
 def parse():
@@ -68,6 +72,25 @@ def parse():
 
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def max_over_ranks(x: float, device=None) -> float:
+    """The largest value of x over all ranks (x itself without a process
+    group): replicas are timed on their own devices and the job takes as long
+    as its slowest rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_stream(nreq: int, rank: int):
+    """Each replica serves its own seeded stream of the same distribution."""
+    from admp_b200 import synthetic
+    return synthetic.serving_stream(nreq, SEED + rank, RATE)
 
 
 # ---------------------------------------------------------------- CPU oracle
@@ -281,7 +304,7 @@ def main():
     from admp_b200 import _lib as L
     from admp_b200.serving import ServingEngine
 
-    stream = synthetic.serving_stream(args.nreq, SEED + rank, RATE)
+    stream = rank_stream(args.nreq, rank)
     total_atoms = sum(r.natoms for r in stream)
     dstream = to_device_requests(stream, dev, torch.float32)
     # pools sized to the stream (capped): all requests fit, so admission never stalls the closed loop
@@ -323,10 +346,7 @@ def main():
     barrier()
     ms = e0.elapsed_time(e1)
     launches = L.launch_count() - launches0
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dev)
     ms_per_step = ms / args.steps
     host_ms = {k: round(v * 1000.0 / args.steps, 3) for k, v in eng.host_time.items()}
     value = args.nreq * world / (ms_per_step / 1000.0)
@@ -353,9 +373,7 @@ def main():
     h2d = (eng.stats["h2d_bytes"] - h0) / (args.steps + 1)
     d2h = (eng.stats["d2h_bytes"] - d0) / (args.steps + 1)
     if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_val = args.nreq * world / float(t.item())
+        e2e_val = args.nreq * world / max_over_ranks(e2e_s, dev)
 
     # open-loop latency at a stated Poisson rate
     lat_rate = args.latency_rate
@@ -397,6 +415,8 @@ def main():
             rf[k] = {"gbs": v["bytes"] / (v["ms"] / 1000.0) / 1e9, "ms_per_launch": v["ms"] / v["launches"],
                      "launches": v["launches"], "share": v["ms"] / tot_ms if tot_ms else None}
     achieved = rf[dom]["gbs"]
+    alg_per_launch = achieved * 1e9 * rf[dom]["ms_per_launch"] / 1e3
+    traffic = TRAFFIC_PER_ALG_BYTE[dom] * alg_per_launch if dom in TRAFFIC_PER_ALG_BYTE else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample = cpu_baseline(stream, args.cpu_seconds)
@@ -422,7 +442,10 @@ def main():
                          "sample": f"first {args.plain_sample} requests vs the FP64 drop-in path "
                                    "(QEq solved to ||P grad||/N < 1e-10)"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": ("ncu DRAM bytes per algorithmic byte of the 400-request stream "
+                                            "x this run's algorithmic bytes per launch") if traffic else None,
+                         "peak_source": peak_src,
                          "kernels": rf},
             "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
             "host_ms_per_step": host_ms,

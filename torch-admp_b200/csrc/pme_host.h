@@ -168,7 +168,8 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
     else
       fft_x_green_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(b, spec, box, acc, ke);
   }
-  prof_end(h, PK_FFT_X_GREEN, 2 * cb, st);
+  // spectrum in and out, plus the cached Green's function (one real per entry) when it is read
+  prof_end(h, PK_FFT_X_GREEN, 2 * cb + (green ? (double)p.spec_elems * sizeof(T) : 0.0), st);
   if (p.slab) {
     h = prof_begin(st);
     if (bs.nblk_y) fft_slab_inv_kernel<T><<<bs.nblk_y, 256, p.smem_slab, st>>>(bs, spec, mesh, p.buf_elems);

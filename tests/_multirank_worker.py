@@ -23,7 +23,9 @@ def main():
     first = [int(r.natoms) for r in stream[:4]]
     gathered = [None] * world
     dist.all_gather_object(gathered, first)
-    print(json.dumps({"rank": rank, "world": world, "max_ms": worst, "streams": gathered}), flush=True)
+    # one file per rank: the ranks share stdout, where their lines may interleave
+    with open(os.path.join(sys.argv[1], f"rank{rank}.json"), "w") as f:
+        json.dump({"rank": rank, "world": world, "max_ms": worst, "streams": gathered}, f)
     dist.destroy_process_group()
 
 

@@ -23,10 +23,10 @@ def _torchrun(args, timeout):
     return subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=timeout)
 
 
-def test_replicas_max_over_ranks_and_own_streams():
-    p = _torchrun([os.path.join(ROOT, "tests", "_multirank_worker.py")], timeout=300)
+def test_replicas_max_over_ranks_and_own_streams(tmp_path):
+    p = _torchrun([os.path.join(ROOT, "tests", "_multirank_worker.py"), str(tmp_path)], timeout=300)
     assert p.returncode == 0, p.stderr[-2000:]
-    lines = [json.loads(ln) for ln in p.stdout.splitlines() if ln.startswith("{")]
+    lines = [json.loads((tmp_path / f"rank{r}.json").read_text()) for r in (0, 1)]
     assert sorted(d["rank"] for d in lines) == [0, 1]
     for d in lines:
         assert d["world"] == 2

@@ -272,20 +272,30 @@ typedef struct admp_pools {
   double* pos64;       /* [A,3] or NULL */
   double* box64;       /* [S,3,3] or NULL */
   void* frac64;        /* [A] double4 scratch, needed with pos64 */
-  /* optional per-slot x-key tables of QEq slots (NULL: not used): the atoms of
-   * a QEq system sorted by their first mesh plane along x (in `sorted`) and
-   * the start of each plane key, which let one thread-block cluster per
-   * system run the whole reciprocal-space matvec of a CG iteration in shared
-   * memory.  Slots whose K0 + 1 exceeds xkey_stride use the mesh passes. */
+  /* optional per-slot x-key tables of QEq slots (used with
+   * ADMP_SERVE_CLUSTER_MATVEC): the atoms of a QEq system sorted by their
+   * first mesh plane along x (in `sorted`) and the start of each plane key,
+   * which let one thread-block cluster per system run the whole
+   * reciprocal-space matvec of a CG iteration in shared memory.  Slots whose
+   * K0 + 1 exceeds xkey_stride use the mesh passes. */
   int* xkey;           /* [S, xkey_stride] */
   int xkey_stride;
+  int flags;           /* ADMP_SERVE_* below */
 } admp_pools;
+
+/* admp_pools.flags: run each CG matvec of QEq slots as one cluster-resident
+ * kernel per system (needs xkey); otherwise the matvec is the atom-parallel
+ * spread, the FFT passes and the atom-parallel gather. */
+#define ADMP_SERVE_CLUSTER_MATVEC 1
 
 size_t admp_serve_slot_state_bytes(void);
 size_t admp_serve_sys_scratch_bytes(int nsys);
 size_t admp_serve_cells_needed(const admp_sys* sys, int nsys);
-/* neighbour rows (CSR) of the listed systems; slot_info[.,2] gets the status
- * (cutoff too large, capacity) and slot_info[.,3] the pair entries needed.   */
+/* neighbour rows of the listed systems: atom a of a system gets the row slot
+ * col[pair_off + a * (pair_cap / natoms) ..] (pstart, pcnt); slot_info[.,2]
+ * gets the status (cutoff too large, non-finite input, or ADMP_ERR_CAPACITY
+ * when a row outgrew its slot) and slot_info[.,3] the pair entries the system
+ * needs after an overflow (natoms x longest row), else 0.                  */
 int admp_serve_neighbors(int dtype, const admp_pools* pools, const admp_sys* sys, int nsys, void* stream);
 /* energy [slot] and forces of the listed systems at the charges in pools->q:
  * PME systems: Ewald real + reciprocal + self + non-neutral (pme.py:261-310);

@@ -140,3 +140,21 @@ def test_cluster_matvec_matches_mesh_passes(cuda, dtype, nmax, qtol, etol):
         assert a.status == 0 and b.status == 0
         assert np.abs(a.charges - b.charges).max() < qtol, (r.natoms, np.abs(a.charges - b.charges).max())
         assert abs(a.energy - b.energy) / abs(b.energy) < etol, (r.natoms, a.energy, b.energy)
+
+
+def test_row_overflow_is_served_again(cuda, stream_and_oracle):
+    """Neighbour rows live in fixed per-atom slots sized from the mean density;
+    a request whose rows outgrow them comes back with ADMP_ERR_CAPACITY and the
+    rows it needs, and the engine serves it again with that capacity."""
+    from admp_b200.serving import ServingEngine
+    reqs, refs = stream_and_oracle
+    eng = ServingEngine(dtype=torch.float64, max_atoms=200_000, max_slots=64, mesh_budget=4_000_000, tol=1e-10)
+    eng._pair_estimate = lambda req: req.natoms * 20 + 64  # far below the ~90 neighbours per atom at rc 6
+    res = {r.rid: r for r in eng.run(reqs, arrivals=False)}
+    assert len(res) == len(reqs)
+    assert eng.stats["retries"] == len(reqs)
+    for r, (E, F, q) in zip(reqs, refs):
+        out = res[r.rid]
+        assert out.status == 0
+        assert abs(out.energy - E) / abs(E) < 1e-9
+        assert np.abs(out.forces - F).max() / np.abs(F).max() < 1e-7

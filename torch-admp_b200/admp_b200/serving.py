@@ -55,7 +55,10 @@ class AdmpPools(ctypes.Structure):
                [("mesh_cap", ctypes.c_longlong), ("spec", _P), ("spec_cap", ctypes.c_longlong), ("acc", _P),
                 ("acc_cap", ctypes.c_int), ("cells", _P), ("cells_cap", ctypes.c_longlong), ("sys_scratch", _P),
                 ("sys_scratch_bytes", ctypes.c_longlong), ("green", _P), ("green_cap", ctypes.c_longlong),
-                ("pos64", _P), ("box64", _P), ("frac64", _P), ("xkey", _P), ("xkey_stride", ctypes.c_int)]
+                ("pos64", _P), ("box64", _P), ("frac64", _P), ("xkey", _P), ("xkey_stride", ctypes.c_int),
+                ("flags", ctypes.c_int)]
+
+SERVE_CLUSTER_MATVEC = 1
 
 # ints per slot of the x-key tables (mesh planes along x + 1)
 XKEY_STRIDE = 1024
@@ -219,12 +222,11 @@ class ServingEngine:
         self.pools.sys_scratch_bytes = t["sys_scratch"].numel()
         self.pools.green_cap = t["green"].numel()
         self.pools.xkey_stride = XKEY_STRIDE
-        if not fused_recip:
-            # no x-key tables: every CG matvec takes the mesh passes (spread, FFT passes, gather).
-            # fused_recip=True runs each matvec as one cluster-resident kernel per system instead
-            # (whole mesh in the shared memory of a 16-CTA cluster); measured slower on the
-            # serving stream (645 vs 194 ms of reciprocal work per 2000-request pass)
-            self.pools.xkey = None
+        # CG matvecs: atom-parallel spread / gather around the FFT passes; fused_recip=True runs each
+        # matvec as one cluster-resident kernel per system instead (whole mesh in the shared memory
+        # of a 16-CTA cluster), measured slower on the serving stream (645 vs 194 ms of
+        # reciprocal work per 2000-request pass)
+        self.pools.flags = SERVE_CLUSTER_MATVEC if fused_recip else 0
         self.greens = _Intervals(t["green"].numel(), 32)
         self.mesh_budget = mesh_budget
         self.atoms = _Intervals(A, 32)
@@ -236,8 +238,10 @@ class ServingEngine:
         self.warm: Dict[object, np.ndarray] = {}
         self.stream = torch.cuda.current_stream(self.dev)
         self.pin = {}
-        self.stats = {"ticks": 0, "launch_calls": 0, "admitted": 0, "h2d_bytes": 0, "d2h_bytes": 0}
+        self.stats = {"ticks": 0, "launch_calls": 0, "admitted": 0, "h2d_bytes": 0, "d2h_bytes": 0, "retries": 0}
         self._fact_cache: Dict[int, tuple] = {}
+        self._pair_grow: Dict[int, tuple] = {}   # pair capacity of requests served again after a row overflow
+        self._retry: Dict[int, tuple] = {}
         self._inflight: List[tuple] = []  # launched work whose results are not read yet, in launch order
         self._zeros = {dt: torch.zeros(3 * 64, dtype=dt, device=self.dev) for dt in (torch.float32, torch.float64)}
         # upload scratch: box rows of one admission on the device, pinned host staging (ring of three)
@@ -286,7 +290,8 @@ class ServingEngine:
             km = auto_kmesh(np.diagonal(self._box_host(req)), self.kappa, self.ethresh)
             f = (req, km, self._mesh_of(km), self._pair_estimate(req))
             self._fact_cache[id(req)] = f
-        return f[1], f[2], f[3]
+        grow = self._pair_grow.get(id(req))
+        return f[1], f[2], (max(f[3], grow[1]) if grow is not None and grow[0] is req else f[3])
 
     def _sys_array(self, items: List[_Active]):
         """ctypes array of the launch descriptors; each request's descriptor is
@@ -369,7 +374,9 @@ class ServingEngine:
                     keep.append((req, tarr))
                     continue
             slot = self.free_slots.pop()
-            admitted.append(_Active(req, slot, aoff, poff, pcap, km, kind, tarr, goff, gn))
+            rt = self._retry.pop(id(req), None)
+            admitted.append(_Active(req, slot, aoff, poff, pcap, km, kind, tarr, goff, gn,
+                                    retries=rt[1] if rt is not None and rt[0] is req else 0))
         keep.sort(key=lambda rt: rt[1])
         self.queue = keep
         if len(self._fact_cache) > 200_000:
@@ -570,6 +577,15 @@ class ServingEngine:
             Fo = Fsrc[off[a.slot]:off[a.slot] + n]
             qo = qsrc[qoff[a.slot]:qoff[a.slot] + n] if a.kind == SYS_QEQ else None
             st = int(ih[a.slot, 2])
+            if st == L.CAPACITY and a.retries < 2:
+                # a neighbour row outgrew its slot: serve the request again with the rows it needs
+                need = int(ih[a.slot, 3])
+                self._pair_grow[id(a.req)] = (a.req, max(2 * a.pair_cap, need + need // 8 + 1024))
+                self._retry[id(a.req)] = (a.req, a.retries + 1)
+                self.queue.append((a.req, a.t_arrival))
+                self.stats["retries"] += 1
+                self._release(a)
+                continue
             it = int(ih[a.slot, 1]) if a.kind == SYS_QEQ else 0
             if host:
                 self.stats["d2h_bytes"] += n * 3 * Fsrc.itemsize + 8 + (n * qsrc.itemsize if qo is not None else 0)

@@ -167,16 +167,14 @@ static int serve_neighbors_impl(const admp_pools* P, const admp_sys* sys, int ns
   sn_setup_kernel<T><<<nsys, 256, 0, st>>>(b, ss, (const T*)P->box, P->box64, P->cells);
   sn_bin_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const T*)P->pos, P->pos64, (V4*)P->frac,
                                                 P->pos64 ? (double4*)P->frac64 : nullptr, P->cell_of, P->cells,
-                                                P->pcnt);
+                                                P->pcnt, P->pstart);
   sn_scan_cells_kernel<<<nsys, 1024, 0, st>>>(ss, P->cells);
   sn_scatter_kernel<<<b.nblk_atom, 256, 0, st>>>(b, ss, P->cell_of, P->cells, P->sorted);
-  sn_pairs_kernel<T, false><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, f64, P->cell_of, P->cells,
-                                                         P->sorted, P->pcnt, nullptr, nullptr);
-  sn_scan_rows_kernel<<<nsys, 1024, 0, st>>>(b, ss, P->pcnt, P->pstart, P->slot_info);
-  sn_pairs_kernel<T, true><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, f64, P->cell_of, P->cells,
-                                                        P->sorted, P->pcnt, P->pstart, P->col);
+  sn_pairs_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, f64, P->cell_of, P->cells, P->sorted,
+                                                  P->pcnt, P->pstart, P->col);
+  sn_export_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, ss, P->slot_info);
   prof_end(hn, PK_NEIGHBORS, -1.0, st);
-  count_launches(8);
+  count_launches(7);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
 }
@@ -262,7 +260,7 @@ static bool cluster_fits(int C, size_t smem) {
 template <typename T>
 static bool build_cluster_plan(const admp_pools* P, const RecipPlan<T>& rp, ClusterPlan& cp) {
   cp.ncls = 0;
-  if (!P->xkey || !P->green || P->xkey_stride <= 0) return false;
+  if (!(P->flags & ADMP_SERVE_CLUSTER_MATVEC) || !P->xkey || !P->green || P->xkey_stride <= 0) return false;
   int pick[kMaxBatch];
   size_t need[kMaxBatch];
   for (int s = 0; s < rp.b.nsys; ++s) {
@@ -393,7 +391,7 @@ static int serve_qeq_init_impl(const admp_pools* P, const admp_sys* sys, int nsy
   // every slot with K0 + 1 <= xkey_stride is sorted, so any later batch of them may take the cluster path
   ClusterPlan cp;
   const bool use_cluster = build_cluster_plan<T>(P, plan, cp);
-  if (P->xkey && P->green && P->xkey_stride > 0) {
+  if ((P->flags & ADMP_SERVE_CLUSTER_MATVEC) && P->xkey && P->green && P->xkey_stride > 0) {
     int mk = 1;
     for (int k = 0; k < nsys; ++k) mk = mk > b.s[k].K0 ? mk : b.s[k].K0;
     xkey_sort_kernel<T><<<nsys, 1024, (mk + 1) * sizeof(int), st>>>(b, (const T*)P->pos, (const T*)P->box,

@@ -96,15 +96,17 @@ template <typename T>
 static __global__ void __launch_bounds__(256)
     sn_bin_kernel(Batch b, SrvSys* __restrict__ ss, const T* __restrict__ pos, const double* __restrict__ pos64,
                   typename Vec4<T>::type* __restrict__ frac, double4* __restrict__ frac64, int* __restrict__ cell_of,
-                  int* __restrict__ cells, int* __restrict__ pcnt) {
+                  int* __restrict__ cells, int* __restrict__ pcnt, long long* __restrict__ pstart) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc& d = b.s[s];
   const SrvSys& S = ss[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
+  const long long row = S.pair_cap / (d.natoms > 0 ? d.natoms : 1);  // fixed row slot per atom
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = d.atom_off + a;
     pcnt[i] = 0;
+    pstart[i] = S.pair_off + (long long)a * row;
     if (S.status) {
       cell_of[i] = -1;
       continue;
@@ -193,22 +195,26 @@ __device__ __forceinline__ void sn_offsets(int nc, int* off, int& n) {
 
 // Thread per binned atom, visited in cell-sorted order so the lanes of a warp
 // share their candidate cells (their candidate loads mostly coalesce or
-// broadcast).  COUNT: pcnt[i]; FILL: col[pstart[i] + k].  Unbinned atoms had
-// pcnt zeroed by sn_bin_kernel.
+// broadcast).  One pass: each atom writes its neighbours into its fixed row
+// slot col[pstart[i] ..] (pstart from sn_bin_kernel, row = pair_cap / natoms)
+// and pcnt[i]; a row that would overflow its slot keeps the first `row`
+// entries, sets the system's status to ADMP_ERR_CAPACITY and raises
+// pair_need to natoms x (longest row).  Unbinned atoms keep pcnt = 0.
 // The cutoff decision is the double-precision one (frac64) whenever frac64 is
 // given: candidates are first tested in T with a margin far above T's
 // rounding error of r^2, and only those inside the margin band around rc^2 or
 // the 1e-4 overlap threshold are re-tested in double.
-template <typename T, bool FILL>
+template <typename T>
 static __global__ void __launch_bounds__(256)
-    sn_pairs_kernel(Batch b, const SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
+    sn_pairs_kernel(Batch b, SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
                     const double4* __restrict__ frac64, const int* __restrict__ cell_of, const int* __restrict__ cells,
                     const int* __restrict__ sorted, int* __restrict__ pcnt, const long long* __restrict__ pstart,
                     int* __restrict__ col) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc& d = b.s[s];
-  const SrvSys& S = ss[s];
+  SrvSys& S = ss[s];
   if (S.status) return;  // sn_bin_kernel left every count of a failed system at zero
+  const long long row = S.pair_cap / (d.natoms > 0 ? d.natoms : 1);
   const int n = S.ncells;
   const int* start = cells + S.cell_off + (n + 1);
   const int nbinned = start[n];
@@ -243,7 +249,7 @@ static __global__ void __launch_bounds__(256)
     const int c0 = ci / (nc1 * nc2), c1 = (ci / nc2) % nc1, c2 = ci % nc2;
     const typename Vec4<T>::type fi = frac[i];
     int cnt = 0;
-    const long long base = FILL ? pstart[i] : 0;
+    const long long base = pstart[i];
     for (int ia = 0; ia < n0; ++ia) {
       int x = c0 + o0[ia];
       T s0 = 0;
@@ -318,51 +324,31 @@ static __global__ void __launch_bounds__(256)
               in = rr < rc2 && rr > 1e-4;
             }
             if (in) {
-              if (FILL) col[base + cnt] = j;
+              if (cnt < row) col[base + cnt] = j;
               ++cnt;
             }
           }
         }
       }
     }
-    if (!FILL) pcnt[i] = cnt;
+    pcnt[i] = cnt < row ? cnt : (int)row;
+    if (cnt > row) {
+      S.status = ADMP_ERR_CAPACITY;  // every writer stores the same value
+      atomicMax(&S.pair_need, (long long)d.natoms * cnt);
+    }
   }
 }
 
-// block per system: row starts pstart = pair_off + exclusive prefix; capacity check
-static __global__ void sn_scan_rows_kernel(Batch b, SrvSys* __restrict__ ss, const int* __restrict__ pcnt,
-                                    long long* __restrict__ pstart, int* __restrict__ slot_info) {
-  __shared__ long long part[1024];
-  const SysDesc& d = b.s[blockIdx.x];
-  SrvSys& S = ss[blockIdx.x];
-  const int n = d.natoms;
-  const int nt = blockDim.x, chunk = (n + nt - 1) / nt;
-  const int b0 = threadIdx.x * chunk, b1 = min(b0 + chunk, n);
-  long long acc = 0;
-  for (int a = b0; a < b1; ++a) acc += pcnt[d.atom_off + a];
-  part[threadIdx.x] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    long long t = 0;
-    for (int k = 0; k < nt; ++k) {
-      const long long v = part[k];
-      part[k] = t;
-      t += v;
-    }
-    S.pair_need = t;
-    if (!S.status && t > S.pair_cap) S.status = ADMP_ERR_CAPACITY;
-    if (slot_info) {
-      int* si = slot_info + 4 * d.box_idx;
-      si[2] = S.status;
-      si[3] = (int)(t < 2147483647LL ? t : 2147483647LL);
-    }
-  }
-  __syncthreads();
-  acc = S.pair_off + part[threadIdx.x];
-  for (int a = b0; a < b1; ++a) {
-    pstart[d.atom_off + a] = acc;
-    acc += pcnt[d.atom_off + a];
-  }
+// thread per system: status and the pair entries a system needs (natoms x
+// longest row when a row overflowed its slot) to slot_info
+static __global__ void sn_export_kernel(Batch b, const SrvSys* __restrict__ ss, int* __restrict__ slot_info) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= b.nsys || !slot_info) return;
+  const SrvSys& S = ss[s];
+  int* si = slot_info + 4 * b.s[s].box_idx;
+  si[2] = S.status;
+  const long long need = S.pair_need;
+  si[3] = (int)(need < 2147483647LL ? need : 2147483647LL);
 }
 
 // minimum-image Cartesian displacement r_j - r_i from wrapped fractional coords

@@ -14,6 +14,22 @@ import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libadmp_b200.so")
+TORCH_OPS_PATH = os.path.join(_HERE, "_torch_ops.so")
+_torch_ops_loaded = False
+
+
+def load_torch_ops() -> None:
+    """Register torch.ops.admp_b200.* (the TorchScript-visible operators over the
+    C ABI, csrc/torch_ops.cpp) once.  Raises ImportError if it is not built."""
+    global _torch_ops_loaded
+    if _torch_ops_loaded:
+        return
+    if not os.path.exists(TORCH_OPS_PATH):
+        raise ImportError(
+            f"admp_b200 torch operators not found at {TORCH_OPS_PATH}; build them with "
+            "`python torch-admp_b200/build.py`.  There is no CPU fallback.")
+    torch.ops.load_library(TORCH_OPS_PATH)
+    _torch_ops_loaded = True
 
 OK, BAD_ARG, CUTOFF, NOT_CONVERGED, WORKSPACE, CUDA, BAD_INDEX, CAPACITY, NONFINITE, MESH = range(10)
 F64, F32 = 0, 1

@@ -3,8 +3,9 @@
 Same forward signature, same shape standardisation to (nframes, ...) and the
 same ValueError messages; units are converted exactly as in the reference
 (positions, box and ds times length_coeff, energy divided by energy_coeff).
+forward and the subclasses' _forward_impl are TorchScript code: the modules
+compile with torch.jit.script (their kernels are torch.ops.admp_b200.*).
 """
-from __future__ import annotations
 
 from abc import ABC, abstractmethod
 from typing import Dict, Optional, Tuple
@@ -24,16 +25,25 @@ class BaseForceModule(torch.nn.Module, ABC):
         _positions, _box, _pairs, _ds, _buffer_scales = self.standardize_input_tensor(
             positions, box, pairs, ds, buffer_scales)
         nf = _positions.size(0)
-        _params = {k: v.reshape(nf, -1) for k, v in params.items()}
+        _params: Dict[str, torch.Tensor] = {}
+        for k, v in params.items():
+            _params[k] = v.reshape(nf, -1)
         lc = self.const_lib.length_coeff
         ec = self.const_lib.energy_coeff
-        energy = self._forward_impl(_positions * lc if lc != 1.0 else _positions,
-                                    (_box * lc if lc != 1.0 else _box) if _box is not None else None,
-                                    _pairs, _ds * lc if lc != 1.0 else _ds, _buffer_scales, _params)
-        return energy / ec if ec != 1.0 else energy
+        if lc != 1.0:
+            _positions = _positions * lc
+            _ds = _ds * lc
+            if _box is not None:
+                _box = _box * lc
+        energy = self._forward_impl(_positions, _box, _pairs, _ds, _buffer_scales, _params)
+        if ec != 1.0:
+            energy = energy / ec
+        return energy
 
     @abstractmethod
-    def _forward_impl(self, positions, box, pairs, ds, buffer_scales, params) -> torch.Tensor:
+    def _forward_impl(self, positions: torch.Tensor, box: Optional[torch.Tensor], pairs: torch.Tensor,
+                      ds: torch.Tensor, buffer_scales: torch.Tensor,
+                      params: Dict[str, torch.Tensor]) -> torch.Tensor:
         """Energy of standardised (nframes, ...) inputs."""
 
     def standardize_input_tensor(self, positions: torch.Tensor, box: Optional[torch.Tensor], pairs: torch.Tensor,
@@ -55,12 +65,12 @@ class BaseForceModule(torch.nn.Module, ABC):
 
         if box is not None:
             if box.dim() == 3:
-                if box.shape[1:] != (3, 3):
+                if box.size(1) != 3 or box.size(2) != 3:
                     raise ValueError(f"box must have shape (nframes, 3, 3), got {box.shape}")
                 if box.size(0) != nframes:
                     raise ValueError(f"box is expected to have {nframes} frame(s), got {box.size(0)}")
             elif box.dim() == 2:
-                if box.shape != (3, 3):
+                if box.size(0) != 3 or box.size(1) != 3:
                     raise ValueError(f"box must have shape (3, 3), got {box.shape}")
                 if nframes != 1:
                     raise ValueError(f"box must include a frame dimension when positions has {nframes} frames")

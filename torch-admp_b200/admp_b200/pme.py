@@ -5,7 +5,6 @@ Constructor arguments, validation messages, energy components
 ``get_rcut`` / ``get_sel`` and ``setup_ewald_parameters`` follow the
 reference.  The energy and every gradient come from the CUDA library.
 """
-from __future__ import annotations
 
 import math
 from typing import Dict, List, Optional, Tuple, Union
@@ -16,7 +15,8 @@ from scipy import special
 
 from . import _lib as L
 from .base_force import BaseForceModule, prep_float
-from .ops import CoulombFn
+
+L.load_torch_ops()  # torch.ops.admp_b200.* used by the forward passes
 
 
 def _auto_kmesh(box_cpu: torch.Tensor, kappa: float, ethresh: float, kmesh, spacing) -> List[List[int]]:
@@ -35,6 +35,10 @@ def _auto_kmesh(box_cpu: torch.Tensor, kappa: float, ethresh: float, kmesh, spac
 
 class CoulombForceModule(BaseForceModule):
     """Coulomb energy with PME (pme.py:24-561)."""
+
+    # TorchScript attribute types (the mesh / spacing settings as lists, empty = automatic)
+    _kmesh_fixed: List[int]
+    _spacing_list: List[float]
 
     def __init__(self, rcut: float, ethresh: float = 1e-5, kspace: bool = True, rspace: bool = True,
                  slab_corr: bool = False, slab_axis: int = 2, units_dict: Optional[Dict] = None,
@@ -76,6 +80,10 @@ class CoulombForceModule(BaseForceModule):
             self.spacing = [float(s) for s in spacing]
         else:
             self.spacing = None
+        self._kmesh_fixed = list(self.kmesh) if self.kmesh is not None else []
+        self._spacing_list = list(self.spacing) if self.spacing is not None else []
+        self.kappa = float(self.kappa)
+        self.ethresh = float(ethresh)
         self.rspace_flag = rspace
         self.slab_corr_flag = slab_corr
         self.slab_axis = slab_axis
@@ -101,35 +109,35 @@ class CoulombForceModule(BaseForceModule):
             return [list(self.kmesh)] * box.shape[0]
         return _auto_kmesh(box.detach().to("cpu", torch.float64), self.kappa, self.ethresh, None, self.spacing)
 
-    def _forward_impl(self, positions, box, pairs, ds, buffer_scales, params):
+    def _forward_impl(self, positions: torch.Tensor, box: Optional[torch.Tensor], pairs: torch.Tensor,
+                      ds: torch.Tensor, buffer_scales: torch.Tensor,
+                      params: Dict[str, torch.Tensor]) -> torch.Tensor:
         nf, na = positions.size(0), positions.size(1)
-        L.require_cuda(positions, "positions")
+        if not positions.is_cuda:
+            raise ValueError("admp_b200 runs on CUDA tensors (there is no CPU path); positions are on "
+                             + str(positions.device))
         dt = positions.dtype
-        charges = prep_float(params["charge"].reshape(nf, na), dt)
-        pos = prep_float(positions, dt)
-        bs = prep_float(buffer_scales, dt)
-        dsc = prep_float(ds, dt)
-        pr = pairs.to(torch.long).contiguous()
-        cfg = {"ke": self.const_lib.dielectric, "kappa": float(self.kappa), "rspace": self.rspace_flag,
-               "kspace": self.kspace_flag, "slab": self.slab_corr_flag, "axis": self.slab_axis}
-        boxc = None
-        if box is not None:
-            boxc = prep_float(box, dt)
-            cfg["kmesh"] = self.kmesh_for(boxc) if self.kspace_flag else [[1, 1, 1]] * nf
-            if self.kspace_flag:
-                self._kmesh = torch.tensor(cfg["kmesh"][-1], dtype=torch.long)
-        E, comps = CoulombFn.apply(pos, boxc, dsc, charges, pr, bs, cfg)
-        c = comps.detach().to(dt)
-        if box is not None:
-            if self.rspace_flag:
-                self.real_energy = c[:, 0]
-            if self.kspace_flag:
-                self.reciprocal_energy = c[:, 1]
-                self.self_energy = c[:, 2]
-                self.non_neutral_energy = c[:, 3]
-            if self.slab_corr_flag:
-                self.slab_corr_energy = c[:, 4]
-        return E
+        charges = params["charge"].reshape(nf, na).to(dt)
+        bs = buffer_scales.to(dt)
+        dsc = ds.to(dt)
+        ke = self.const_lib.dielectric
+        if box is None:
+            return torch.ops.admp_b200.coulomb_obc(pairs, dsc, bs, charges, ke)
+        out = torch.ops.admp_b200.coulomb_pbc(positions.to(dt), box.to(dt), pairs, dsc, bs, charges, self.kappa,
+                                              self._kmesh_fixed, self._spacing_list, self.ethresh, ke,
+                                              self.rspace_flag, self.kspace_flag, self.slab_corr_flag,
+                                              self.slab_axis)
+        c = out[1].to(dt)
+        if self.kspace_flag:
+            self._kmesh = out[2][-1]
+            self.reciprocal_energy = c[:, 1]
+            self.self_energy = c[:, 2]
+            self.non_neutral_energy = c[:, 3]
+        if self.rspace_flag:
+            self.real_energy = c[:, 0]
+        if self.slab_corr_flag:
+            self.slab_corr_energy = c[:, 4]
+        return out[0]
 
 
 def setup_ewald_parameters(rcut: float, box=None, threshold: float = 1e-5, spacing: Optional[float] = None,

@@ -13,7 +13,6 @@ through the implicit function theorem: the backward runs a second CG with the
 same operator (the adjoint) and contracts it with mixed second derivatives
 obtained from the energy kernels (polarisation identity).
 """
-from __future__ import annotations
 
 import ctypes
 from typing import Dict, List, Optional, Tuple, Union
@@ -24,7 +23,9 @@ from . import _lib as L
 from .base_force import BaseForceModule, prep_float
 from .ops import DampingFn, SiteFn, coulomb_pbc, damping_raw
 from .pme import CoulombForceModule
-from .utils import vector_projection, vector_projection_coeff_matrix
+from .utils import calc_pgrads, vector_projection, vector_projection_coeff_matrix
+
+L.load_torch_ops()  # torch.ops.admp_b200.* used by the forward passes
 
 
 class GaussianDampingForceModule(BaseForceModule):
@@ -33,15 +34,14 @@ class GaussianDampingForceModule(BaseForceModule):
     def __init__(self, units_dict: Optional[Dict] = None) -> None:
         BaseForceModule.__init__(self, units_dict)
 
-    def _forward_impl(self, positions, box, pairs, ds, buffer_scales, params):
+    def _forward_impl(self, positions: torch.Tensor, box: Optional[torch.Tensor], pairs: torch.Tensor,
+                      ds: torch.Tensor, buffer_scales: torch.Tensor,
+                      params: Dict[str, torch.Tensor]) -> torch.Tensor:
         nf, na = positions.size(0), positions.size(1)
         dt = positions.dtype
-        L.require_cuda(positions, "positions")
-        q = prep_float(params["charge"].reshape(nf, na), dt)
-        eta = params["eta"].reshape(nf, na) * self.const_lib.length_coeff
-        eta = prep_float(eta, dt)
-        return DampingFn.apply(prep_float(ds, dt), q, eta, pairs.to(torch.long).contiguous(),
-                               prep_float(buffer_scales, dt), self.const_lib.dielectric)
+        q = params["charge"].reshape(nf, na).to(dt)
+        eta = (params["eta"].reshape(nf, na) * self.const_lib.length_coeff).to(dt)
+        return torch.ops.admp_b200.damping(ds.to(dt), q, eta, pairs, buffer_scales.to(dt), self.const_lib.dielectric)
 
 
 class SiteForceModule(BaseForceModule):
@@ -50,15 +50,16 @@ class SiteForceModule(BaseForceModule):
     def __init__(self, units_dict: Optional[Dict] = None) -> None:
         BaseForceModule.__init__(self, units_dict)
 
-    def _forward_impl(self, positions, box, pairs, ds, buffer_scales, params):
+    def _forward_impl(self, positions: torch.Tensor, box: Optional[torch.Tensor], pairs: torch.Tensor,
+                      ds: torch.Tensor, buffer_scales: torch.Tensor,
+                      params: Dict[str, torch.Tensor]) -> torch.Tensor:
         nf, na = positions.size(0), positions.size(1)
         dt = positions.dtype
-        L.require_cuda(positions, "positions")
         ec = self.const_lib.energy_coeff
-        chi = prep_float(params["chi"].reshape(nf, na) * ec, dt)
-        hard = prep_float(params["hardness"].reshape(nf, na) * ec, dt)
-        q = prep_float(params["charge"].reshape(nf, na), dt)
-        return SiteFn.apply(q, chi, hard)
+        chi = (params["chi"].reshape(nf, na) * ec).to(dt)
+        hard = (params["hardness"].reshape(nf, na) * ec).to(dt)
+        q = params["charge"].reshape(nf, na).to(dt)
+        return torch.ops.admp_b200.site(q, chi, hard)
 
 
 class QEqForceModule(BaseForceModule):
@@ -95,19 +96,34 @@ class QEqForceModule(BaseForceModule):
     def get_sel(self):
         return self.sel
 
-    def _forward_impl(self, positions, box, pairs, ds, buffer_scales, params):
+    def _forward_impl(self, positions: torch.Tensor, box: Optional[torch.Tensor], pairs: torch.Tensor,
+                      ds: torch.Tensor, buffer_scales: torch.Tensor,
+                      params: Dict[str, torch.Tensor]) -> torch.Tensor:
         energy = torch.zeros(positions.size(0), device=positions.device, dtype=positions.dtype)
         for model in self.submodels.values():
-            energy = energy + model._forward_impl(positions, box, pairs, ds, buffer_scales, params)
+            energy = energy + model(positions, box, pairs, ds, buffer_scales, params)
         return energy
 
-    def func_energy(self, charges, positions, box, chi, hardness, eta, pairs, ds, buffer_scales):
+    @torch.jit.export
+    def func_energy(self, charges: torch.Tensor, positions: torch.Tensor, box: Optional[torch.Tensor],
+                    chi: torch.Tensor, hardness: torch.Tensor, eta: torch.Tensor, pairs: torch.Tensor,
+                    ds: torch.Tensor, buffer_scales: torch.Tensor) -> torch.Tensor:
         """Total QEq energy (qeq.py:408-458)."""
-        params = {"charge": charges, "chi": chi, "hardness": hardness, "eta": eta}
+        params: Dict[str, torch.Tensor] = {"charge": charges, "chi": chi, "hardness": hardness, "eta": eta}
         energy = torch.zeros(1, device=positions.device, dtype=positions.dtype)
         for model in self.submodels.values():
             energy = energy + model(positions, box, pairs, ds, buffer_scales, params)
         return energy
+
+    @torch.jit.export
+    def optimality(self, charges: torch.Tensor, positions: torch.Tensor, box: Optional[torch.Tensor],
+                   chi: torch.Tensor, hardness: torch.Tensor, eta: torch.Tensor, pairs: torch.Tensor,
+                   ds: torch.Tensor, buffer_scales: torch.Tensor, constraint_matrix: torch.Tensor,
+                   coeff_matrix: torch.Tensor) -> torch.Tensor:
+        """Normalised projected gradient ||P dE/dq|| / N, ~0 at the optimal charges (qeq.py:714-764)."""
+        energy = self.func_energy(charges, positions, box, chi, hardness, eta, pairs, ds, buffer_scales)
+        pgrads = calc_pgrads(energy, charges, constraint_matrix, coeff_matrix)
+        return torch.norm(pgrads) / charges.shape[0]
 
     # -- solver plumbing -------------------------------------------------
     def _flags(self) -> int:

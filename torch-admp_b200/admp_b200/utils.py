@@ -4,9 +4,8 @@ Unit handling follows the reference: inputs in the user's length/energy
 units are converted to Angstrom / eV (ASE conventions, CODATA 2014 values as
 used by ``ase.units``) before the kernels run.
 """
-from __future__ import annotations
 
-from typing import Dict, Optional
+from typing import Dict, List, Optional
 
 import numpy as np
 import torch
@@ -31,8 +30,8 @@ class TorchConstants(torch.nn.Module):
 
     def __init__(self, units_dict: Optional[Dict] = None):
         super().__init__()
-        self.pi = np.pi
-        self.sqrt_pi = np.sqrt(np.pi)
+        self.pi = float(np.pi)
+        self.sqrt_pi = float(np.sqrt(np.pi))
         units_dict = units_dict or {}
         user_energy = units_dict.get("energy", "eV")
         user_length = units_dict.get("length", "Ang")
@@ -44,10 +43,10 @@ class TorchConstants(torch.nn.Module):
             energy_coeff = _ASE_UNITS[user_energy]
         else:
             raise ValueError(f"Unknown energy unit: {user_energy}")
-        self.length_coeff = _ASE_UNITS[user_length]
-        self.energy_coeff = energy_coeff
-        self.epsilon = EPSILON
-        self.dielectric = DIELECTRIC
+        self.length_coeff = float(_ASE_UNITS[user_length])
+        self.energy_coeff = float(energy_coeff)
+        self.epsilon = float(EPSILON)
+        self.dielectric = float(DIELECTRIC)
 
 
 def safe_inverse(x: torch.Tensor, threshold: float = 1e-8) -> torch.Tensor:
@@ -80,12 +79,14 @@ def vector_projection(vector_in: torch.Tensor, constraint_matrix: torch.Tensor,
 def calc_grads(t_out: torch.Tensor, t_in: torch.Tensor) -> torch.Tensor:
     """d(sum t_out)/d t_in -- utils.py:85-112."""
     assert t_in.requires_grad, "Input tensor requires grad"
-    (g,) = torch.autograd.grad([t_out], [t_in], grad_outputs=[torch.ones_like(t_out)], retain_graph=True)
+    grad_outputs: List[Optional[torch.Tensor]] = [torch.ones_like(t_out)]
+    g = torch.autograd.grad([t_out], [t_in], grad_outputs=grad_outputs, retain_graph=True)[0]
     assert g is not None
     return g
 
 
-def calc_pgrads(t_out, t_in, constraint_matrix, coeff_matrix):
+def calc_pgrads(t_out: torch.Tensor, t_in: torch.Tensor, constraint_matrix: torch.Tensor,
+                coeff_matrix: torch.Tensor) -> torch.Tensor:
     """Projected gradient -- utils.py:116-149."""
     g = calc_grads(t_out, t_in).reshape(-1, 1)
     residual = -constraint_matrix @ g

@@ -77,6 +77,45 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
     return LIB
 
 
+TORCH_OPS_SRC = os.path.join(CSRC, "torch_ops.cpp")
+TORCH_OPS = os.path.join(OUT_DIR, "_torch_ops.so")
+
+
+def build_torch_ops(force: bool = False, verbose: bool = False) -> str:
+    """TorchScript-visible operators (torch.ops.admp_b200.*, csrc/torch_ops.cpp):
+    a C++ torch extension linked against libadmp_b200.so (rpath $ORIGIN)."""
+    import torch
+    from torch.utils import cpp_extension as ce
+    abi = int(torch._C._GLIBCXX_USE_CXX11_ABI)
+    incs = ce.include_paths(device_type="cuda") if "device_type" in ce.include_paths.__code__.co_varnames \
+        else ce.include_paths(cuda=True)
+    libs = ce.library_paths(device_type="cuda") if "device_type" in ce.library_paths.__code__.co_varnames \
+        else ce.library_paths(cuda=True)
+    flags = ["-O2", "-std=c++17", "-shared", "-fPIC", f"-D_GLIBCXX_USE_CXX11_ABI={abi}",
+             "-DTORCH_EXTENSION_NAME=_torch_ops", f"-I{INCLUDE}"] + [f"-I{d}" for d in incs]
+    h = hashlib.sha256()
+    for f in (TORCH_OPS_SRC, os.path.join(INCLUDE, "admp_b200.h")):
+        h.update(open(f, "rb").read())
+    h.update((" ".join(flags) + torch.__version__).encode())
+    dig = h.hexdigest()
+    stamp = os.path.join(OUT_DIR, ".torch_ops.sha256")
+    if not force and os.path.exists(TORCH_OPS) and os.path.exists(stamp) and open(stamp).read().strip() == dig:
+        return TORCH_OPS
+    tmp = TORCH_OPS + ".tmp"
+    cmd = (["g++"] + flags + [TORCH_OPS_SRC, "-o", tmp] + [f"-L{d}" for d in libs] +
+           ["-lc10", "-lc10_cuda", "-ltorch", "-ltorch_cpu", "-ltorch_cuda", f"-L{OUT_DIR}", "-ladmp_b200",
+            "-Wl,-rpath,$ORIGIN"] + [f"-Wl,-rpath,{d}" for d in libs])
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"torch ops build failed:\n{r.stdout}\n{r.stderr[-6000:]}")
+    os.replace(tmp, TORCH_OPS)
+    with open(stamp, "w") as f:
+        f.write(dig)
+    return TORCH_OPS
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
@@ -84,4 +123,5 @@ if __name__ == "__main__":
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args()
     print(build(force=a.force, debug=a.debug, verbose=a.verbose))
+    print(build_torch_ops(force=a.force, verbose=a.verbose))
     sys.exit(0)

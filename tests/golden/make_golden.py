@@ -309,6 +309,14 @@ ELECTRODE_CASES = {
     "lmp_conp_slab_3d": (False, True, [(0, 108, 20.0, "conp"), (108, 216, 0.0, "conp")], True),
     "lmp_conp_interface_2d_bias": (True, False, [(0, 108, 20.0, "conp"), (108, 216, 0.0, "conp")], True),
     "lmp_conq_interface_2d_pzc": (True, False, [(0, 216, 0.0, "conq")], False),
+    # the remaining LAMMPS fixtures of test_electrode_conp.py / test_electrode_conq.py, with their settings
+    "lmp_conp_interface_2d_pzc": (True, False, [(0, 108, 0.0, "conp"), (108, 216, 0.0, "conp")], True),
+    "lmp_conp_interface_3d_pzc": (False, True, [(0, 108, 0.0, "conp"), (108, 216, 0.0, "conp")], True),
+    "lmp_conp_interface_3d_bias": (False, True, [(0, 108, 20.0, "conp"), (108, 216, 0.0, "conp")], True),
+    "lmp_conq_interface_3d_pzc": (False, False, [(0, 216, 0.0, "conq")], False),
+    "lmp_conq_interface_2d_edl": (True, False, [(0, 216, -10.0, "conq")], False),
+    "lmp_conq_interface_3d_edl": (False, False, [(0, 216, -10.0, "conq")], False),
+    "lmp_conq_interface_2d_bias": (True, False, [(0, 108, -10.0, "conq"), (108, 216, 10.0, "conq")], False),
 }
 
 

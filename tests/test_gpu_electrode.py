@@ -11,7 +11,11 @@ from _gpu_helpers import T, rel
 pytestmark = pytest.mark.gpu
 
 CASES = [("electrode_conp_slab_2d", 5e-5), ("electrode_conp_slab_3d", 5e-5),
-         ("electrode_conp_interface_2d_bias", 5e-4), ("electrode_conq_interface_2d_pzc", 5e-4)]
+         ("electrode_conp_interface_2d_bias", 5e-4), ("electrode_conq_interface_2d_pzc", 5e-4),
+         ("electrode_conp_interface_2d_pzc", 5e-4), ("electrode_conp_interface_3d_pzc", 5e-4),
+         ("electrode_conp_interface_3d_bias", 5e-4), ("electrode_conq_interface_3d_pzc", 5e-4),
+         ("electrode_conq_interface_2d_edl", 5e-4), ("electrode_conq_interface_3d_edl", 5e-4),
+         ("electrode_conq_interface_2d_bias", 5e-4)]
 
 
 @pytest.mark.parametrize("name,tol", CASES)

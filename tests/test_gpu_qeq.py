@@ -146,3 +146,24 @@ def test_implicit_adjoint_vs_finite_differences(cuda):
             fd = (lp - lm) / (2 * h)
             an = g[idx].item()
             assert abs(fd - an) < 1e-6 + 1e-4 * abs(fd), (arr_name, k, fd, an)
+
+
+@pytest.mark.parametrize("groups", [2, 3])
+def test_qeq_cg_group_constraints_match_kkt(cuda, groups):
+    """Several constraint rows that are not the all-ones row (charge of each of
+    `groups` atom groups fixed): the projected CG and the dense KKT solve give
+    the same charges, and every group carries its prescribed charge."""
+    from admp_b200.qeq import matinv_optimize, pgrad_optimize
+    d = golden("qeq_water_small")
+    m, pos, box, pairs, ds, bs, chi, hd, eta, _, _ = setup(d, cuda, 20, eps=1e-10, max_iter=2000)
+    n = pos.shape[0]
+    edges = np.linspace(0, n, groups + 1).astype(int)
+    C = torch.zeros(groups, n, dtype=torch.float64, device=cuda)
+    for g in range(groups):
+        C[g, edges[g]:edges[g + 1]] = 1.0
+    b = torch.tensor(np.linspace(-1.5, 1.0, groups), dtype=torch.float64, device=cuda)
+    _, q_cg = pgrad_optimize(m, torch.zeros(n, dtype=torch.float64, device=cuda), pos, box, chi, hd, eta, pairs, ds,
+                             bs, C, b, method="quadratic", reinit_q=True)
+    _, q_kkt = matinv_optimize(m, pos, box, chi, hd, eta, pairs, ds, bs, C, b)
+    np.testing.assert_allclose((C @ q_cg.detach()).cpu().numpy(), b.cpu().numpy(), atol=1e-9)
+    assert (q_cg.detach() - q_kkt.detach()).abs().max().item() < 1e-7

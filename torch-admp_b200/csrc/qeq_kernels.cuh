@@ -54,7 +54,7 @@ __device__ __forceinline__ bool sys_done(const CGScal* sc, int s) {
 // row of the total-charge constraint.
 template <typename T>
 __device__ __forceinline__ double cval(const T* C, int c, long long cstride, int i) {
-  return C ? cval(C, c, cstride, i) : 1.0;
+  return C ? (double)C[(long long)c * cstride + i] : 1.0;
 }
 
 // Setup per atom: diag_i, z_i, chi_eff_i; per system (block 0 thread 0 of the

@@ -35,7 +35,7 @@ from . import _lib as L
 from .utils import DIELECTRIC
 
 SYS_PME, SYS_QEQ = 0, 1
-MAX_PER_LAUNCH = 128
+MAX_PER_LAUNCH = 256
 
 
 class AdmpSys(ctypes.Structure):
@@ -314,7 +314,7 @@ class ServingEngine:
         return (AdmpSys * len(items)).from_buffer_copy(b"".join(a.packed for a in items))
 
     def _chunks(self, items: List[_Active]):
-        """Split into launches of <= 128 systems whose meshes fit the scratch budget."""
+        """Split into launches of <= MAX_PER_LAUNCH systems whose meshes fit the scratch budget."""
         out, cur, mesh = [], [], 0
         for a in items:
             m = self._mesh_of(a.kmesh)

@@ -13,7 +13,7 @@ constexpr int kOrder = 6;          // PME B-spline order (pme.py:167-169 fixes 6
 constexpr int kStencil = 216;      // 6^3 mesh points per atom
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kSqrtPi = 1.77245385090551602730;
-constexpr int kMaxBatch = 128;     // systems per launch descriptor
+constexpr int kMaxBatch = 256;     // systems per launch descriptor (by-value kernel parameter, < 32 KB)
 
 template <typename T>
 struct Cplx {

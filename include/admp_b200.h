@@ -170,6 +170,38 @@ int admp_nblist_fill(int dtype, int pbc, int natoms, const void* pos, const void
                      long long* buffer_scales, long long capacity, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Neighbour list over periodic images for any cutoff, including rc above   */
+/* half the box: replaces dp_nblist (nblist.py:33-93) with its               */
+/* make_extended_pairs / make_local_pairs / make_ds (nblist.py:140-240).    */
+/* Pairs (i, j, n) with |r_j - r_i + n.B| <= rc: first every i < j image    */
+/* (buffer scale 1), then every self image (i, i, n != 0) (scale 1/2).      */
+/* nnei >= 0 keeps each atom's nnei nearest images, as the per-atom `sel`   */
+/* truncation of the list dp_nblist is built from (ties at the nnei-th      */
+/* distance are all kept); nnei < 0 keeps all.  Two phases, one workspace:  */
+/*   admp_image_nblist_count -> *n_ij, *n_ii (host; synchronises `stream`), */
+/*                              *n_truncated = atoms that hit nnei;         */
+/*   admp_image_nblist_fill  -> pairs [n_ij+n_ii, 2] int64 (i-major), and   */
+/*                              shifts [n_ij+n_ii, 3] int32 image vectors n.*/
+/* pbc = 0 (box may be NULL): plain pairs within rc, no images.             */
+/* Pair distances and their backward for pairs with image shifts:           */
+/* ds = |r_j - r_i + n.B|; the box gradient is sum_p n_p (x) dL/d(dr_p).     */
+/* ------------------------------------------------------------------------ */
+size_t admp_image_nblist_workspace_size(int natoms);
+int admp_image_nblist_count(int dtype, int pbc, int natoms, const void* pos, const void* box,
+                            double cutoff, int nnei, void* workspace, size_t workspace_bytes,
+                            long long* n_ij, long long* n_ii, int* n_truncated, void* stream);
+int admp_image_nblist_fill(int dtype, int pbc, int natoms, const void* pos, const void* box,
+                           double cutoff, void* workspace, size_t workspace_bytes, long long* pairs,
+                           int* shifts, long long capacity, void* stream);
+int admp_image_pair_distances(int dtype, int natoms, long long npairs, const long long* pairs,
+                              const int* shifts, const void* pos, const void* box, void* ds,
+                              void* stream);
+int admp_image_pair_distances_backward(int dtype, int natoms, long long npairs,
+                                       const long long* pairs, const int* shifts, const void* pos,
+                                       const void* box, const void* grad_ds, void* grad_pos,
+                                       void* grad_box, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Matrix-free projected CG solve of the QEq charges: replaces               */
 /* pgrad_optimize / QEqForceModule.solve_pgrad (qeq.py:609-712, 1117-1270)   */
 /* and the quadratic / LBFGS minimisers (qeq.py:1273-1527).  Minimises       */

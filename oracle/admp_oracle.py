@@ -146,6 +146,69 @@ def nblist_obc(pos: np.ndarray, rc: float) -> np.ndarray:
     return np.argwhere(m).astype(np.int64)
 
 
+def image_nblist(pos: np.ndarray, box: Optional[np.ndarray], rc: float, nnei: int):
+    """dp_nblist's pair set for any cutoff -- nblist.py:33-93 with
+    make_extended_pairs / make_local_pairs / make_ds (nblist.py:140-240).
+
+    The per-atom list comes from deepmd-kit's (pt backend, not vendored with
+    the reference and not pinned by it) extend_input_and_build_neighbor_list,
+    whose published behaviour is restated here: coordinates are wrapped into
+    the cell, ghost images are made within ceil(rc / h_d) cells along each
+    axis d (h_d the cell height), each local atom's list holds every image
+    (the atom itself excluded) with r <= rc, sorted by distance and cut to
+    its first `nnei` entries (`sel`).  make_local_pairs then keeps the i < j
+    entries (scale 1) followed by the self images i == j (scale 1/2), and
+    make_ds takes |x_j' - x_i| from the extended coordinates.
+
+    Returns (pairs [P,2] int64, shifts [P,3] int64 with
+    ds = |r_j - r_i + shift.box| for the caller's unwrapped positions,
+    ds [P], buffer_scales [P]).  Within each block the order here is (i, j,
+    image); the reference orders by distance, so tests compare sorted sets.
+    """
+    pos = np.asarray(pos, np.float64).reshape(-1, 3)
+    n = pos.shape[0]
+    if box is None:
+        bx = np.eye(3)
+        f = pos.copy()
+        k = np.zeros((n, 3), np.int64)
+        m = np.zeros(3, np.int64)
+    else:
+        bx = np.asarray(box, np.float64).reshape(3, 3)
+        x = pos @ np.linalg.inv(bx)
+        k = np.floor(x).astype(np.int64)
+        f = x - k
+        V = abs(np.linalg.det(bx))
+        h = np.array([V / np.linalg.norm(np.cross(bx[(d + 1) % 3], bx[(d + 2) % 3])) for d in range(3)])
+        m = np.ceil(rc / h).astype(np.int64)
+    imgs = np.stack(np.meshgrid(*[np.arange(-m[d], m[d] + 1) for d in range(3)], indexing="ij"), -1).reshape(-1, 3)
+    rows_ij, rows_ii = [], []
+    for i in range(n):
+        df = f[None, :, :] - f[i][None, None, :] + imgs[:, None, :]          # [nimg, n, 3]
+        r = np.linalg.norm(df @ bx, axis=-1)
+        r[np.all(imgs == 0, axis=1), i] = np.inf
+        ii, jj = np.nonzero(r <= rc)
+        sel = np.argsort(r[ii, jj], kind="stable")
+        if nnei >= 0 and sel.size > nnei:
+            rth = r[ii, jj][sel[nnei - 1]] if nnei > 0 else -1.0
+            keep = r[ii, jj] <= rth
+            ii, jj = ii[keep], jj[keep]
+        shift = imgs[ii] + k[i][None, :] - k[jj]
+        for a, j, s in zip(ii, jj, shift):
+            if j > i:
+                rows_ij.append((i, j, *s, r[a, j]))
+            elif j == i:
+                rows_ii.append((i, j, *s, r[a, j]))
+    rows_ij.sort(key=lambda t: t[:5])
+    rows_ii.sort(key=lambda t: t[:5])
+    rows = rows_ij + rows_ii
+    if not rows:
+        return (np.zeros((0, 2), np.int64), np.zeros((0, 3), np.int64), np.zeros(0), np.zeros(0))
+    arr = np.array([t[:5] for t in rows], np.int64)
+    ds = np.array([t[5] for t in rows])
+    bs = np.concatenate([np.ones(len(rows_ij)), np.full(len(rows_ii), 0.5)])
+    return arr[:, :2], arr[:, 2:5], ds, bs
+
+
 # --------------------------------------------------------------------------
 # Ewald parameters
 # --------------------------------------------------------------------------

@@ -45,7 +45,8 @@ EXPORTS = [
     "admp_launch_count", "admp_profile_enable", "admp_profile_read", "admp_serve_slot_state_bytes",
     "admp_serve_sys_scratch_bytes", "admp_serve_cells_needed", "admp_serve_neighbors", "admp_serve_energy_forces",
     "admp_serve_qeq_init", "admp_serve_qeq_iterate", "admp_serve_qeq_finish", "admp_pme_recip_noalloc_max_scratch",
-    "admp_pme_recip_noalloc",
+    "admp_pme_recip_noalloc", "admp_image_nblist_workspace_size", "admp_image_nblist_count",
+    "admp_image_nblist_fill", "admp_image_pair_distances", "admp_image_pair_distances_backward",
 ]
 PROFILE_KERNELS = ["spread", "fft_z_fwd", "fft_y_fwd", "fft_x_green", "fft_y_inv", "fft_z_inv", "gather", "pair_ef",
                    "csr_spmv", "neighbors", "cg_vector", "recip_fused"]
@@ -79,6 +80,11 @@ _SIGS = {
     "admp_launch_count": (_ll, []),
     "admp_pme_recip_noalloc_max_scratch": (_sz, []),
     "admp_pme_recip_noalloc": (_i, [_i, _i, _i, _ip, _vp, _vp, _vp, _d, _d, _vp, _vp, _vp, _vp, _vp]),
+    "admp_image_nblist_workspace_size": (_sz, [_i]),
+    "admp_image_nblist_count": (_i, [_i, _i, _i, _vp, _vp, _d, _i, _vp, _sz, _llp, _llp, _ip, _vp]),
+    "admp_image_nblist_fill": (_i, [_i, _i, _i, _vp, _vp, _d, _vp, _sz, _vp, _vp, _ll, _vp]),
+    "admp_image_pair_distances": (_i, [_i, _i, _ll, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "admp_image_pair_distances_backward": (_i, [_i, _i, _ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "admp_profile_enable": (_i, [_i]),
     "admp_profile_read": (_i, [_dp, _llp, _dp, _i]),
 }

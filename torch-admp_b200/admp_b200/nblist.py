@@ -1,9 +1,14 @@
-"""TorchNeighborList on the GPU cell list (nblist.py:268-617, check_cutoff :620-660).
+"""Neighbour lists on the GPU.
 
+TorchNeighborList (nblist.py:268-617, check_cutoff :620-660) on a cell list:
 ``forward(positions, box)`` returns the full pair list (both orders, sorted by
 (i, j)) and stores ``pairs``, ``buffer_scales`` (1 if i < j) and ``ds``; ``ds``
 is differentiable with respect to positions and box (hand-written backward),
 as in the reference, so forces can flow through the caller's distances.
+
+dp_nblist / vesin_nblist (nblist.py:33-138) for cutoffs above half the box:
+one pair per periodic image within the cutoff, built by the image kernels,
+with distances differentiable through the stored image shifts.
 """
 from __future__ import annotations
 
@@ -12,7 +17,7 @@ from typing import Optional
 import torch
 
 from . import _lib as L
-from .ops import PairDistanceFn, neighbor_pairs
+from .ops import ImagePairDistanceFn, PairDistanceFn, image_neighbor_pairs, neighbor_pairs
 
 
 def check_cutoff(box: torch.Tensor, cutoff: float) -> None:
@@ -79,3 +84,56 @@ class TorchNeighborList(torch.nn.Module):
 
     def get_ds(self):
         return self.ds
+
+
+def _image_list(positions: torch.Tensor, box: Optional[torch.Tensor], rcut: float, nnei: int):
+    if rcut <= 0.0:
+        raise ValueError(f"rcut must be positive, got {rcut}")
+    L.require_cuda(positions, "positions")
+    pos = positions.reshape(-1, 3)
+    b = box.reshape(3, 3).to(pos.dtype) if box is not None else None
+    pairs, shifts, n_ij, _ = image_neighbor_pairs(pos.detach().contiguous(),
+                                                  b.detach().contiguous() if b is not None else None,
+                                                  float(rcut), int(nnei))
+    ds = ImagePairDistanceFn.apply(pos.contiguous(), b.contiguous() if b is not None else None, pairs, shifts)
+    return pairs, shifts, ds, n_ij
+
+
+def dp_nblist(positions: torch.Tensor, box: Optional[torch.Tensor], nnei: int, rcut: float):
+    """Pairs over periodic images (nblist.py:33-93): returns (pairs, ds, buffer_scales).
+
+    pairs holds every image (i, j) with i < j and r <= rcut (buffer scale 1),
+    followed by every self image (i, i) of an atom (scale 1/2); each atom
+    keeps its ``nnei`` nearest images, the ``sel`` cut of the per-atom list
+    dp_nblist is built from (atoms with a tie at the nnei-th distance keep all
+    tied images).  ds is differentiable in positions and box.  Within each
+    block pairs are ordered by (i, j, image) rather than by distance.
+    """
+    pairs, _shifts, ds, n_ij = _image_list(positions, box, rcut, nnei)
+    buffer_scales = torch.ones(pairs.shape[0], device=pairs.device)
+    buffer_scales[n_ij:] = 0.5
+    return pairs, ds, buffer_scales
+
+
+def vesin_nblist(positions: torch.Tensor, box: torch.Tensor, rcut: float):
+    """Half list over periodic images (nblist.py:96-138): returns (pairs, ds, buffer_scales).
+
+    Same image pairs as dp_nblist, but each self image is kept once (of the
+    two opposite shifts n and -n, the one whose first non-zero component is
+    positive) and every buffer scale is 1 -- the half-list convention.
+    """
+    pairs, shifts, ds, n_ij = _image_list(positions, box, rcut, -1)
+    if pairs.shape[0] > n_ij:
+        s = shifts[n_ij:].to(torch.long)
+        first = torch.where(s[:, 0] != 0, s[:, 0], torch.where(s[:, 1] != 0, s[:, 1], s[:, 2]))
+        keep = torch.cat([torch.ones(n_ij, dtype=torch.bool, device=pairs.device), first > 0])
+        pairs, ds = pairs[keep], ds[keep]
+    return pairs, ds, torch.ones_like(ds)
+
+
+def sort_pairs(pairs: torch.Tensor) -> torch.Tensor:
+    """Rows sorted by (first, second) index (nblist.py:243-264)."""
+    idx = torch.argsort(pairs[:, 1])
+    pairs = pairs[idx]
+    idx = torch.argsort(pairs[:, 0], stable=True)
+    return pairs[idx]

@@ -242,3 +242,62 @@ def neighbor_pairs(pos: torch.Tensor, box: Optional[torch.Tensor], cutoff: float
         L.check(lib.admp_nblist_fill(dt, pbc, N, L.ptr(pos), L.ptr(box), float(cutoff), L.ptr(ws), nbytes,
                                      L.ptr(pairs), L.ptr(bs), P, st), "neighbour list fill")
     return pairs, bs
+
+
+class ImagePairDistanceFn(torch.autograd.Function):
+    """ds = |r_j - r_i + n.B| for pairs with integer image shifts n (make_ds, nblist.py:212-240)."""
+
+    @staticmethod
+    def forward(ctx, pos, box, pairs, shifts):
+        lib = L.load()
+        dt = L.dtype_code(pos.dtype)
+        P = pairs.shape[0]
+        ds = torch.empty(P, dtype=pos.dtype, device=pos.device)
+        L.check(lib.admp_image_pair_distances(dt, pos.shape[0], P, L.ptr(pairs), L.ptr(shifts), L.ptr(pos),
+                                              L.ptr(box), L.ptr(ds), L.stream_of(pos.device)), "pair distances")
+        ctx.save_for_backward(pos, box if box is not None else torch.empty(0, device=pos.device), pairs, shifts)
+        ctx.has_box = box is not None
+        return ds
+
+    @staticmethod
+    def backward(ctx, gds):
+        pos, box, pairs, shifts = ctx.saved_tensors
+        lib = L.load()
+        dt = L.dtype_code(pos.dtype)
+        gpos = torch.zeros_like(pos) if ctx.needs_input_grad[0] else None
+        gbox = torch.zeros_like(box) if (ctx.has_box and ctx.needs_input_grad[1]) else None
+        if gpos is not None or gbox is not None:
+            L.check(lib.admp_image_pair_distances_backward(dt, pos.shape[0], pairs.shape[0], L.ptr(pairs),
+                                                           L.ptr(shifts), L.ptr(pos),
+                                                           L.ptr(box) if ctx.has_box else None,
+                                                           L.ptr(gds.contiguous()), L.ptr(gpos), L.ptr(gbox),
+                                                           L.stream_of(pos.device)), "pair distances backward")
+        return gpos, gbox, None, None
+
+
+def image_neighbor_pairs(pos: torch.Tensor, box: Optional[torch.Tensor], cutoff: float, nnei: int):
+    """Pairs over periodic images (dp_nblist's pair set, nblist.py:33-93, 173-209).
+
+    Returns pairs [P,2] int64 (i < j images, then self images (i, i)), image
+    shifts [P,3] int32, the number of i < j pairs and the number of atoms
+    whose list was cut to their nnei nearest images."""
+    import ctypes
+    lib = L.load()
+    dev = pos.device
+    dt = L.dtype_code(pos.dtype)
+    N = pos.shape[0]
+    st = L.stream_of(dev)
+    nbytes = lib.admp_image_nblist_workspace_size(N)
+    ws = L.workspace(nbytes, dev)
+    n_ij, n_ii, ntr = ctypes.c_longlong(0), ctypes.c_longlong(0), ctypes.c_int(0)
+    pbc = 1 if box is not None else 0
+    L.check(lib.admp_image_nblist_count(dt, pbc, N, L.ptr(pos), L.ptr(box), float(cutoff), int(nnei), L.ptr(ws),
+                                        nbytes, ctypes.byref(n_ij), ctypes.byref(n_ii), ctypes.byref(ntr), st),
+            "image neighbour list")
+    P = int(n_ij.value) + int(n_ii.value)
+    pairs = torch.empty((P, 2), dtype=torch.long, device=dev)
+    shifts = torch.empty((P, 3), dtype=torch.int32, device=dev)
+    if P > 0:
+        L.check(lib.admp_image_nblist_fill(dt, pbc, N, L.ptr(pos), L.ptr(box), float(cutoff), L.ptr(ws), nbytes,
+                                           L.ptr(pairs), L.ptr(shifts), P, st), "image neighbour list fill")
+    return pairs, shifts, int(n_ij.value), int(ntr.value)

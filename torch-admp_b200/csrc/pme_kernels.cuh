@@ -226,24 +226,35 @@ __global__ void __launch_bounds__(256) spread_kernel(Batch b, const T* __restric
   T* M = mesh + d.mesh_off;
   WarpStencil<T, false> ws;
   ws.carve(dsm + warp * WarpStencil<T, false>::bytes());
-  const int y0 = lane / 6, z0 = lane % 6, y1 = (lane + 32) / 6, z1 = (lane + 32) % 6;
+  // columns 0..31 of an atom: lane = 6 y + z; the last four columns (y 5, z 2..5) of eight
+  // atoms at once: lane -> atom lane / 4, z 2 + lane % 4
+  const int y0 = lane / 6, z0 = lane % 6, jt = lane >> 2, zt = 2 + (lane & 3);
   for (int a0 = a_begin + warp * 32; a0 < a_end; a0 += nw * 32) {
     warp_build_stencil<T, false>(ws, d, g, pos, q, order, a0, a_end, lane);
     const int na = min(32, a_end - a0);
-    for (int j = 0; j < na; ++j) {
-      const T qa = ws.q[j];
-      if (qa == T(0)) continue;
-      const T* w = ws.w + j * 18;
-      const int* ox = ws.ox + j * 6;
-      const int by = ws.byz[2 * j], bz = ws.byz[2 * j + 1];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (h == 1 && lane >= 4) break;
-        const int yy = h ? y1 : y0, zz = h ? z1 : z0;
-        const T wyz = qa * w[6 + yy] * w[12 + zz];
-        const int oyz = wrap_up(by + yy, d.K1) * d.K2 + wrap_up(bz + zz, d.K2);
+    for (int j0 = 0; j0 < na; j0 += 8) {
+      const int j1 = min(j0 + 8, na);
+      for (int j = j0; j < j1; ++j) {
+        const T qa = ws.q[j];
+        if (qa == T(0)) continue;
+        const T* w = ws.w + j * 18;
+        const int* ox = ws.ox + j * 6;
+        const T wyz = qa * w[6 + y0] * w[12 + z0];
+        const int oyz = wrap_up(ws.byz[2 * j] + y0, d.K1) * d.K2 + wrap_up(ws.byz[2 * j + 1] + z0, d.K2);
 #pragma unroll
         for (int dx = 0; dx < 6; ++dx) atomicAdd(M + ox[dx] + oyz, w[dx] * wyz);
+      }
+      const int j = j0 + jt;
+      if (j < j1) {
+        const T qa = ws.q[j];
+        if (qa != T(0)) {
+          const T* w = ws.w + j * 18;
+          const int* ox = ws.ox + j * 6;
+          const T wyz = qa * w[6 + 5] * w[12 + zt];
+          const int oyz = wrap_up(ws.byz[2 * j] + 5, d.K1) * d.K2 + wrap_up(ws.byz[2 * j + 1] + zt, d.K2);
+#pragma unroll
+          for (int dx = 0; dx < 6; ++dx) atomicAdd(M + ox[dx] + oyz, w[dx] * wyz);
+        }
       }
     }
     __syncwarp();
@@ -744,7 +755,8 @@ __global__ void __launch_bounds__(256) gather_kernel(Batch b, const T* __restric
   const int K[3] = {d.K0, d.K1, d.K2};
   WarpStencil<T, FORCES> ws;
   ws.carve(dsm + warp * WarpStencil<T, FORCES>::bytes());
-  const int y0 = lane / 6, z0 = lane % 6, y1 = (lane + 32) / 6, z1 = (lane + 32) % 6;
+  // column mapping as in spread_kernel: columns 0..31 per atom, the last four of eight atoms at once
+  const int y0 = lane / 6, z0 = lane % 6, jt = lane >> 2, zt = 2 + (lane & 3);
   double wf[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) wf[k] = 0.0;
@@ -752,17 +764,13 @@ __global__ void __launch_bounds__(256) gather_kernel(Batch b, const T* __restric
     warp_build_stencil<T, FORCES>(ws, d, g, pos, FORCES ? q : nullptr, order, a0, a_end, lane);
     const int na = min(32, a_end - a0);
     T my_pot = 0, my_g0 = 0, my_g1 = 0, my_g2 = 0;
-    for (int j = 0; j < na; ++j) {
-      const T* w = ws.w + j * 18;
-      const int* ox = ws.ox + j * 6;
-      const int by = ws.byz[2 * j], bz = ws.byz[2 * j + 1];
-      T pot = 0, g0 = 0, g1 = 0, g2 = 0;
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (h == 1 && lane >= 4) break;
-        const int yy = h ? y1 : y0, zz = h ? z1 : z0;
-        const T wy = w[6 + yy], wz = w[12 + zz];
-        const int oyz = wrap_up(by + yy, d.K1) * d.K2 + wrap_up(bz + zz, d.K2);
+    for (int j0 = 0; j0 < na; j0 += 8) {
+      const int j1 = min(j0 + 8, na);
+      for (int j = j0; j < j1; ++j) {
+        const T* w = ws.w + j * 18;
+        const int* ox = ws.ox + j * 6;
+        const T wy = w[6 + y0], wz = w[12 + z0];
+        const int oyz = wrap_up(ws.byz[2 * j] + y0, d.K1) * d.K2 + wrap_up(ws.byz[2 * j + 1] + z0, d.K2);
         T sw = 0, sdw = 0;
 #pragma unroll
         for (int dx = 0; dx < 6; ++dx) {
@@ -770,24 +778,64 @@ __global__ void __launch_bounds__(256) gather_kernel(Batch b, const T* __restric
           sw += f * w[dx];
           if (FORCES) sdw += f * ws.dw[j * 18 + dx];
         }
-        pot += sw * wy * wz;
+        T pot = sw * wy * wz, g0 = 0, g1 = 0, g2 = 0;
+        pot = warp_sum(pot);
         if (FORCES) {
-          g0 += sdw * wy * wz;
-          g1 += sw * ws.dw[j * 18 + 6 + yy] * wz;
-          g2 += sw * wy * ws.dw[j * 18 + 12 + zz];
+          g0 = warp_sum(sdw * wy * wz);
+          g1 = warp_sum(sw * ws.dw[j * 18 + 6 + y0] * wz);
+          g2 = warp_sum(sw * wy * ws.dw[j * 18 + 12 + z0]);
+        }
+        if (lane == j) {
+          my_pot = pot;
+          my_g0 = g0;
+          my_g1 = g1;
+          my_g2 = g2;
         }
       }
-      pot = warp_sum(pot);
-      if (FORCES) {
-        g0 = warp_sum(g0);
-        g1 = warp_sum(g1);
-        g2 = warp_sum(g2);
+      // the last four columns of atoms j0 .. j1-1, reduced over each atom's four lanes
+      T pot = 0, g0 = 0, g1 = 0, g2 = 0;
+      const int j = j0 + jt;
+      if (j < j1) {
+        const T* w = ws.w + j * 18;
+        const int* ox = ws.ox + j * 6;
+        const T wy = w[6 + 5], wz = w[12 + zt];
+        const int oyz = wrap_up(ws.byz[2 * j] + 5, d.K1) * d.K2 + wrap_up(ws.byz[2 * j + 1] + zt, d.K2);
+        T sw = 0, sdw = 0;
+#pragma unroll
+        for (int dx = 0; dx < 6; ++dx) {
+          const T f = M[ox[dx] + oyz];
+          sw += f * w[dx];
+          if (FORCES) sdw += f * ws.dw[j * 18 + dx];
+        }
+        pot = sw * wy * wz;
+        if (FORCES) {
+          g0 = sdw * wy * wz;
+          g1 = sw * ws.dw[j * 18 + 6 + 5] * wz;
+          g2 = sw * wy * ws.dw[j * 18 + 12 + zt];
+        }
       }
-      if (lane == j) {
-        my_pot = pot;
-        my_g0 = g0;
-        my_g1 = g1;
-        my_g2 = g2;
+#pragma unroll
+      for (int o = 1; o < 4; o <<= 1) {
+        pot += __shfl_xor_sync(0xffffffffu, pot, o);
+        if (FORCES) {
+          g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+          g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+          g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+        }
+      }
+      // lane j0 + k takes the sums of atom j0 + k from lane 4 k
+      const int src = 4 * ((lane - j0) & 7);
+      pot = __shfl_sync(0xffffffffu, pot, src);
+      if (FORCES) {
+        g0 = __shfl_sync(0xffffffffu, g0, src);
+        g1 = __shfl_sync(0xffffffffu, g1, src);
+        g2 = __shfl_sync(0xffffffffu, g2, src);
+      }
+      if (lane >= j0 && lane < j1) {
+        my_pot += pot;
+        my_g0 += g0;
+        my_g1 += g1;
+        my_g2 += g2;
       }
     }
     if (lane < na) {

@@ -5,7 +5,7 @@
 //   pair_ef   : warp per atom over its CSR row: Ewald real space (pme.py:312-349)
 //               and Gaussian damping (qeq.py:104-119) energy, force, potential
 //   csr_coef  : QEq real-space matrix entries ke (erfc(kappa r) - erfc(r / 2 eta_ij)) / r
-//   csr_spmv  : Hp += J_real p, warp per row
+//   csr_spmv  : Hp += J_real p, eight lanes per row
 //   sys_terms : per-system self / non-neutral / damping-self / site energies
 #pragma once
 
@@ -489,7 +489,13 @@ static __global__ void __launch_bounds__(256)
   }
 }
 
-// Hp[i] += sum_k coef[k] p[col[k]]  (warp per row)
+// Hp[i] += sum_k coef[k] p[col[k]].  Eight lanes per row, four rows per warp
+// at a time; each lane issues the loads of up to kSpmvUnroll entries of its
+// row before using any of them, so a row costs about three dependent memory
+// latencies (row start, entries, gathered p) instead of three per 32
+// entries: the kernel is bound by the latency of those chains, not by bytes.
+constexpr int kSpmvLanes = 8;
+constexpr int kSpmvUnroll = 12;
 template <typename T>
 static __global__ void __launch_bounds__(256)
     csr_spmv_kernel(Batch b, const long long* __restrict__ pstart, const int* __restrict__ pcnt,
@@ -498,17 +504,37 @@ static __global__ void __launch_bounds__(256)
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc& d = b.s[s];
   if (done && done[(size_t)d.box_idx * done_stride]) return;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = threadIdx.x & (kSpmvLanes - 1);
+  const int grp = threadIdx.x / kSpmvLanes, ngrp = blockDim.x / kSpmvLanes;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
-  for (int a = a0 + warp; a < a1; a += blockDim.x >> 5) {
-    const int i = d.atom_off + a;
+  // every lane runs the same number of loop trips (shuffles below use the full mask)
+  for (int base = a0; base < a1; base += ngrp) {
+    const int a = base + grp;
+    const bool row = a < a1;
+    const int i = d.atom_off + (row ? a : a0);
     const long long st = pstart[i];
-    const int n = pcnt[i];
+    const int n = row ? pcnt[i] : 0;
     T acc = 0;
-    for (int k = lane; k < n; k += 32) acc += coef[st + k] * p[col[st + k]];
-    acc = warp_sum(acc);
-    if (lane == 0) Hp[i] += acc;
+    for (int k0 = 0; k0 < n; k0 += kSpmvLanes * kSpmvUnroll) {
+      int c[kSpmvUnroll];
+      T w[kSpmvUnroll];
+#pragma unroll
+      for (int u = 0; u < kSpmvUnroll; ++u) {
+        const int k = k0 + sub + u * kSpmvLanes;
+        const bool ok = k < n;
+        c[u] = ok ? col[st + k] : -1;
+        w[u] = ok ? coef[st + k] : T(0);
+      }
+      T v[kSpmvUnroll];
+#pragma unroll
+      for (int u = 0; u < kSpmvUnroll; ++u) v[u] = c[u] >= 0 ? p[c[u]] : T(0);
+#pragma unroll
+      for (int u = 0; u < kSpmvUnroll; ++u) acc += w[u] * v[u];
+    }
+#pragma unroll
+    for (int o = kSpmvLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (row && sub == 0) Hp[i] += acc;
   }
 }
 

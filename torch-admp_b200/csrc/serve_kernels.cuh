@@ -193,13 +193,52 @@ __device__ __forceinline__ void sn_offsets(int nc, int* off, int& n) {
   }
 }
 
-// Thread per binned atom, visited in cell-sorted order so the lanes of a warp
-// share their candidate cells (their candidate loads mostly coalesce or
-// broadcast).  One pass: each atom writes its neighbours into its fixed row
-// slot col[pstart[i] ..] (pstart from sn_bin_kernel, row = pair_cap / natoms)
-// and pcnt[i]; a row that would overflow its slot keeps the first `row`
-// entries, sets the system's status to ADMP_ERR_CAPACITY and raises
-// pair_need to natoms x (longest row).  Unbinned atoms keep pcnt = 0.
+// Asynchronous 16-byte global -> shared copies (cp.async, sm_80+): the
+// issuing warp does not wait for them until cp.async.wait_group.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Neighbour cells of a home cell, as a flat sequence of candidate chunks of
+// up to 32 atoms (warp-uniform state).
+struct SnChunk {
+  int q;   // neighbour cell (index into the warp's table), nq when past the end
+  int t0;  // first sorted position of the chunk
+};
+__device__ __forceinline__ SnChunk sn_first(const int* tb_begin, const int* tb_end, int nq) {
+  SnChunk c{0, nq > 0 ? tb_begin[0] : 0};
+  while (c.q < nq && c.t0 >= tb_end[c.q]) {
+    ++c.q;
+    if (c.q < nq) c.t0 = tb_begin[c.q];
+  }
+  return c;
+}
+__device__ __forceinline__ SnChunk sn_next(SnChunk c, const int* tb_begin, const int* tb_end, int nq) {
+  if (c.q >= nq) return c;
+  c.t0 += 32;
+  while (c.q < nq && c.t0 >= tb_end[c.q]) {
+    ++c.q;
+    if (c.q < nq) c.t0 = tb_begin[c.q];
+  }
+  return c;
+}
+
+// Warp per home cell: lane l takes home atom l of the cell (chunks of 32).
+// The warp streams the atoms of the (up to 27) neighbour cells through a
+// double buffer in shared memory, 32 at a time: the sorted indices of chunk
+// k + 2 are loaded and the positions of chunk k + 1 copied asynchronously
+// while every lane tests its atom against chunk k with broadcast loads, so
+// the search runs at instruction rate instead of waiting on dependent global
+// loads per candidate.  Rows keep the order of a per-atom scan: neighbour
+// cells in (x, y, z) offset order, candidates in sorted order.  One pass:
+// each atom writes its neighbours into its fixed row slot col[pstart[i] ..]
+// (pstart from sn_bin_kernel, row = pair_cap / natoms) and pcnt[i]; a row
+// that would overflow its slot keeps the first `row` entries, sets the
+// system's status to ADMP_ERR_CAPACITY and raises pair_need to natoms x
+// (longest row).  Unbinned atoms keep pcnt = 0.
 // The cutoff decision is the double-precision one (frac64) whenever frac64 is
 // given: candidates are first tested in T with a margin far above T's
 // rounding error of r^2, and only those inside the margin band around rc^2 or
@@ -210,22 +249,29 @@ static __global__ void __launch_bounds__(256)
                     const double4* __restrict__ frac64, const int* __restrict__ cell_of, const int* __restrict__ cells,
                     const int* __restrict__ sorted, int* __restrict__ pcnt, const long long* __restrict__ pstart,
                     int* __restrict__ col) {
+  typedef typename Vec4<T>::type V4;
+  constexpr int kV4Chunks = sizeof(V4) / 16;
+  __shared__ __align__(16) V4 cand[8][2][32];
+  __shared__ int cand_j[8][2][32];
+  __shared__ int tb_begin[8][27], tb_end[8][27], tb_shift[8][27];
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc& d = b.s[s];
   SrvSys& S = ss[s];
   if (S.status) return;  // sn_bin_kernel left every count of a failed system at zero
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const long long row = S.pair_cap / (d.natoms > 0 ? d.natoms : 1);
   const int n = S.ncells;
   const int* start = cells + S.cell_off + (n + 1);
-  const int nbinned = start[n];
-  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
-  const int a1 = min(a0 + b.apb, nbinned);
   const double rc2 = S.rc * S.rc;
   const int nc0 = S.nc[0], nc1 = S.nc[1], nc2 = S.nc[2];
-  int o0[3], o1[3], o2[3], n0, n1, n2;
-  sn_offsets(nc0, o0, n0);
-  sn_offsets(nc1, o1, n1);
-  sn_offsets(nc2, o2, n2);
+  int n0, n1, n2;
+  {
+    int o[3];
+    sn_offsets(nc0, o, n0);
+    sn_offsets(nc1, o, n1);
+    sn_offsets(nc2, o, n2);
+  }
+  const int nq = n0 * n1 * n2;
   T bt[9];
   double bsum = 0.0;
 #pragma unroll
@@ -243,50 +289,89 @@ static __global__ void __launch_bounds__(256)
   const bool ortho = S.b[1] == 0.0 && S.b[2] == 0.0 && S.b[3] == 0.0 && S.b[5] == 0.0 && S.b[6] == 0.0 &&
                      S.b[7] == 0.0;
   const int* srt = sorted + d.atom_off;
-  for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
-    const int i = srt[a];
-    const int ci = cell_of[i];
-    const int c0 = ci / (nc1 * nc2), c1 = (ci / nc2) % nc1, c2 = ci % nc2;
-    const typename Vec4<T>::type fi = frac[i];
-    int cnt = 0;
-    const long long base = pstart[i];
-    for (int ia = 0; ia < n0; ++ia) {
-      int x = c0 + o0[ia];
-      T s0 = 0;
-      if (x < 0) {
-        x += nc0;
-        s0 = T(-1);
-      } else if (x >= nc0) {
-        x -= nc0;
-        s0 = T(1);
-      }
-      for (int ib = 0; ib < n1; ++ib) {
-        int y = c1 + o1[ib];
-        T s1 = 0;
-        if (y < 0) {
-          y += nc1;
-          s1 = T(-1);
-        } else if (y >= nc1) {
-          y -= nc1;
-          s1 = T(1);
+  int* tbb = tb_begin[warp];
+  int* tbe = tb_end[warp];
+  int* tbs = tb_shift[warp];
+  const int nwarps_sys = ((d.natoms + b.apb - 1) / b.apb) * nw;
+  for (int c = (blockIdx.x - d.blk_atom) * nw + warp; c < n; c += nwarps_sys) {
+    const int h_begin = start[c], h_end = start[c + 1];
+    if (h_begin >= h_end) continue;
+    const int c0 = c / (nc1 * nc2), c1 = (c / nc2) % nc1, c2 = c % nc2;
+    // table of neighbour cells: lane q < nq takes offset q in (x, y, z) order
+    __syncwarp();
+    if (lane < nq) {
+      const int q2 = lane % n2, q1 = (lane / n2) % n1, q0 = lane / (n1 * n2);
+      int xyz[3] = {c0 + (n0 == 3 ? q0 - 1 : q0), c1 + (n1 == 3 ? q1 - 1 : q1), c2 + (n2 == 3 ? q2 - 1 : q2)};
+      const int ncs[3] = {nc0, nc1, nc2};
+      int code = 0;
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        int sh = 0;
+        if (xyz[e] < 0) {
+          xyz[e] += ncs[e];
+          sh = -1;
+        } else if (xyz[e] >= ncs[e]) {
+          xyz[e] -= ncs[e];
+          sh = 1;
         }
-        for (int ic = 0; ic < n2; ++ic) {
-          int z = c2 + o2[ic];
-          T s2 = 0;
-          if (z < 0) {
-            z += nc2;
-            s2 = T(-1);
-          } else if (z >= nc2) {
-            z -= nc2;
-            s2 = T(1);
-          }
+        code |= (sh + 1) << (2 * e);
+      }
+      const int cc = (xyz[0] * nc1 + xyz[1]) * nc2 + xyz[2];
+      tbb[lane] = start[cc];
+      tbe[lane] = start[cc + 1];
+      tbs[lane] = code;
+    }
+    __syncwarp();
+    for (int h0 = h_begin; h0 < h_end; h0 += 32) {
+      const bool home = h0 + lane < h_end;
+      const int i = home ? srt[h0 + lane] : -1;
+      V4 fi;
+      if (home) {
+        fi = frac[i];
+      } else {
+        fi.x = fi.y = fi.z = fi.w = T(0);
+      }
+      const long long base = home ? pstart[i] : 0;
+      int cnt = 0;
+      // prologue: indices of chunks 0 and 1, positions of chunk 0 in flight
+      SnChunk cur = sn_first(tbb, tbe, nq);
+      SnChunk nxt = sn_next(cur, tbb, tbe, nq);
+      int bsel = 0;
+      {
+        const int j = (cur.q < nq && cur.t0 + lane < tbe[cur.q]) ? srt[cur.t0 + lane] : -1;
+        cand_j[warp][0][lane] = j;
+        if (j >= 0)
+#pragma unroll
+          for (int h = 0; h < kV4Chunks; ++h)
+            cp_async16(reinterpret_cast<char*>(&cand[warp][0][lane]) + 16 * h,
+                       reinterpret_cast<const char*>(frac + j) + 16 * h);
+        cp_async_commit();
+      }
+      int jn = (nxt.q < nq && nxt.t0 + lane < tbe[nxt.q]) ? srt[nxt.t0 + lane] : -1;
+      while (cur.q < nq) {
+        const SnChunk nxt2 = sn_next(nxt, tbb, tbe, nq);
+        // positions of the next chunk into the other buffer (one group per trip, empty at the end)
+        cand_j[warp][bsel ^ 1][lane] = jn;
+        if (jn >= 0)
+#pragma unroll
+          for (int h = 0; h < kV4Chunks; ++h)
+            cp_async16(reinterpret_cast<char*>(&cand[warp][bsel ^ 1][lane]) + 16 * h,
+                       reinterpret_cast<const char*>(frac + jn) + 16 * h);
+        cp_async_commit();
+        const int jn2 = (nxt2.q < nq && nxt2.t0 + lane < tbe[nxt2.q]) ? srt[nxt2.t0 + lane] : -1;
+        cp_async_wait1();  // this chunk's copies have landed
+        __syncwarp();
+        if (home) {
+          const int code = tbs[cur.q];
+          const T s0 = T((code & 3) - 1), s1 = T(((code >> 2) & 3) - 1), s2 = T(((code >> 4) & 3) - 1);
           const T g0 = s0 - fi.x, g1 = s1 - fi.y, g2 = s2 - fi.z;
-          const int cc = (x * nc1 + y) * nc2 + z;
-          const int t1 = start[cc + 1];
-          for (int t = start[cc]; t < t1; ++t) {
-            const int j = srt[t];
+          const int nt = min(32, tbe[cur.q] - cur.t0);
+          const V4* cw = cand[warp][bsel];
+          const int* cj = cand_j[warp][bsel];
+          for (int k = 0; k < nt; ++k) {
+            const int j = cj[k];
             if (j == i) continue;
-            const typename Vec4<T>::type fj = frac[j];
+            const V4 fj = cw[k];
             T f0 = fj.x + g0, f1 = fj.y + g1, f2 = fj.z + g2;
             if (!fast) {
               f0 -= floor(f0 + T(0.5));
@@ -329,12 +414,19 @@ static __global__ void __launch_bounds__(256)
             }
           }
         }
+        __syncwarp();  // this buffer is refilled two trips later
+        cur = nxt;
+        nxt = nxt2;
+        jn = jn2;
+        bsel ^= 1;
       }
-    }
-    pcnt[i] = cnt < row ? cnt : (int)row;
-    if (cnt > row) {
-      S.status = ADMP_ERR_CAPACITY;  // every writer stores the same value
-      atomicMax(&S.pair_need, (long long)d.natoms * cnt);
+      if (home) {
+        pcnt[i] = cnt < row ? cnt : (int)row;
+        if (cnt > row) {
+          S.status = ADMP_ERR_CAPACITY;  // every writer stores the same value
+          atomicMax(&S.pair_need, (long long)d.natoms * cnt);
+        }
+      }
     }
   }
 }

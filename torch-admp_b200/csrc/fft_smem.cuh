@@ -52,6 +52,22 @@ __device__ __forceinline__ int fdiv(int x, const FastDiv& f) {
   return f.d > 1 ? (int)__umulhi((unsigned)x, f.m) : x;
 }
 
+// Item idx of a stage -> (line l, butterfly j).  LINE_FAST: consecutive items
+// take consecutive lines.  NL > 0 (a power of two) is the line count known at
+// compile time, so the split is a mask and a shift.
+template <bool LINE_FAST, int NL>
+__device__ __forceinline__ void split_item(int idx, const FastDiv& f, int& l, int& j) {
+  if (LINE_FAST && NL > 0) {
+    l = idx & (NL - 1);
+    j = idx / NL;
+  } else {
+    const int qd = fdiv(idx, f);
+    const int rm = idx - qd * f.d;
+    l = LINE_FAST ? rm : qd;
+    j = LINE_FAST ? qd : rm;
+  }
+}
+
 // W[e] = exp(-2 pi i e / n), e in [0, n); computed in double.
 template <typename T>
 __device__ __forceinline__ void make_twiddles(Cplx<T>* W, int n) {
@@ -78,10 +94,10 @@ __device__ __forceinline__ void make_twiddles(Cplx<T>* W, int n) {
 // ones.  Step 1 twiddles and folds the inputs (in -> out, in the butterfly's
 // own output slots), step 2 forms the output pairs (out -> in), so the result
 // of this stage is left in `in`.
-template <typename T, bool LINE_FAST, bool WARP>
+template <typename T, bool LINE_FAST, bool WARP, bool INV, int NL>
 __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
                                              int nl, int n, int ls, int es, int Ns, int r,
-                                             const Cplx<T>* __restrict__ W, bool inverse, int tid, int nthr) {
+                                             const Cplx<T>* __restrict__ W, int tid, int nthr) {
   const int nb = n / r;
   const int h = (r - 1) >> 1;
   const int scale = n / (Ns * r);
@@ -89,10 +105,8 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
   const FastDiv f_split = fast_div(LINE_FAST ? nl : nb), f_ns = fast_div(Ns), f_items = fast_div(nl * nb);
   const int total1 = nl * nb;
   for (int idx = tid; idx < total1; idx += nthr) {
-    const int qd = fdiv(idx, f_split);
-    const int rm = idx - qd * f_split.d;
-    const int l = LINE_FAST ? rm : qd;
-    const int j = LINE_FAST ? qd : rm;
+    int l, j;
+    split_item<LINE_FAST, NL>(idx, f_split, l, j);
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
     const Cplx<T>* src = in + (int)l * ls;
@@ -104,7 +118,7 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
       const Cplx<T> c = src[(int)(j + (r - u) * nb) * es];
       const Cplx<T> wa = W[scale * k * u];
       const Cplx<T> wc = W[scale * k * (r - u)];
-      const T way = inverse ? -wa.y : wa.y, wcy = inverse ? -wc.y : wc.y;
+      const T way = INV ? -wa.y : wa.y, wcy = INV ? -wc.y : wc.y;
       const T ax = a.x * wa.x - a.y * way, ay = a.x * way + a.y * wa.x;
       const T cx = c.x * wc.x - c.y * wcy, cy = c.x * wcy + c.y * wc.x;
       Cplx<T> sv, dv;
@@ -124,10 +138,8 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
   for (int idx = tid; idx < total2; idx += nthr) {
     const int kk = fdiv(idx, f_items);
     const int it = idx - kk * f_items.d;
-    const int qd = fdiv(it, f_split);
-    const int rm = it - qd * f_split.d;
-    const int l = LINE_FAST ? rm : qd;
-    const int j = LINE_FAST ? qd : rm;
+    int l, j;
+    split_item<LINE_FAST, NL>(it, f_split, l, j);
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
     const Cplx<T>* src = out + (int)l * ls;
@@ -161,7 +173,7 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
       by -= dv.y * w.y;
     }
     // forward: X_k = A - i B, X_{r-k} = A + i B (inverse: signs swapped); -i B = (B.y, -B.x)
-    const T ibx = inverse ? -by : by, iby = inverse ? bx : -bx;
+    const T ibx = INV ? -by : by, iby = INV ? bx : -bx;
     Cplx<T> X1, X2;
     X1.x = ax + ibx;
     X1.y = ay + iby;
@@ -175,20 +187,18 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
 // Radix-3 and radix-5 stages: one thread per butterfly, inputs twiddled from
 // the table, then the small DFT with the exact cosines / sines of 2 pi / 3 and
 // 2 pi / 5 (sign of the sines flips for the inverse transform).
-template <typename T, bool LINE_FAST, int R>
+template <typename T, bool LINE_FAST, int R, bool INV, int NL>
 __device__ __forceinline__ void stockham_r35(const Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
                                              int nl, int n, int ls, int es, int Ns,
-                                             const Cplx<T>* __restrict__ W, bool inverse, int tid, int nthr) {
+                                             const Cplx<T>* __restrict__ W, int tid, int nthr) {
   const int nb = n / R;
   const int total = nl * nb;
   const int scale = n / (Ns * R);
   const FastDiv f_split = fast_div(LINE_FAST ? nl : nb), f_ns = fast_div(Ns);
-  const T sg = inverse ? T(-1) : T(1);
+  const T sg = INV ? T(-1) : T(1);
   for (int idx = tid; idx < total; idx += nthr) {
-    const int qd = fdiv(idx, f_split);
-    const int rm = idx - qd * f_split.d;
-    const int l = LINE_FAST ? rm : qd;
-    const int j = LINE_FAST ? qd : rm;
+    int l, j;
+    split_item<LINE_FAST, NL>(idx, f_split, l, j);
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
     const Cplx<T>* src = in + (int)l * ls;
@@ -200,7 +210,7 @@ __device__ __forceinline__ void stockham_r35(const Cplx<T>* __restrict__ in, Cpl
         v[0] = x;
       } else {
         const Cplx<T> w = W[scale * k * t];
-        const T wy = inverse ? -w.y : w.y;
+        const T wy = INV ? -w.y : w.y;
         v[t].x = x.x * w.x - x.y * wy;
         v[t].y = x.x * wy + x.y * w.x;
       }
@@ -246,19 +256,17 @@ __device__ __forceinline__ void stockham_r35(const Cplx<T>* __restrict__ in, Cpl
 }
 
 // Radix-4 stage, one thread per butterfly (4 outputs).
-template <typename T, bool LINE_FAST>
+template <typename T, bool LINE_FAST, bool INV, int NL>
 __device__ __forceinline__ void stockham_r4(const Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
                                             int nl, int n, int ls, int es, int Ns,
-                                            const Cplx<T>* __restrict__ W, bool inverse, int tid, int nthr) {
+                                            const Cplx<T>* __restrict__ W, int tid, int nthr) {
   const int nb = n >> 2;
   const int total = nl * nb;
   const int scale = n / (Ns * 4);
   const FastDiv f_split = fast_div(LINE_FAST ? nl : nb), f_ns = fast_div(Ns);
   for (int idx = tid; idx < total; idx += nthr) {
-    const int qd = fdiv(idx, f_split);
-    const int rm = idx - qd * f_split.d;
-    const int l = LINE_FAST ? rm : qd;
-    const int j = LINE_FAST ? qd : rm;
+    int l, j;
+    split_item<LINE_FAST, NL>(idx, f_split, l, j);
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
     const Cplx<T>* src = in + (int)l * ls;
@@ -270,7 +278,7 @@ __device__ __forceinline__ void stockham_r4(const Cplx<T>* __restrict__ in, Cplx
         v[0] = x;
       } else {
         Cplx<T> w = W[scale * k * t];
-        T wy = inverse ? -w.y : w.y;
+        T wy = INV ? -w.y : w.y;
         v[t].x = x.x * w.x - x.y * wy;
         v[t].y = x.x * wy + x.y * w.x;
       }
@@ -281,8 +289,8 @@ __device__ __forceinline__ void stockham_r4(const Cplx<T>* __restrict__ in, Cplx
     T cx = v[1].x + v[3].x, cy = v[1].y + v[3].y;
     T dx = v[1].x - v[3].x, dy = v[1].y - v[3].y;
     // (-i) * d = (dy, -dx); (+i) * d = (-dy, dx)
-    T mdx = inverse ? -dy : dy;
-    T mdy = inverse ? dx : -dx;
+    T mdx = INV ? -dy : dy;
+    T mdy = INV ? dx : -dx;
     const int base = jq * Ns * 4 + k;
     Cplx<T>* dst = out + (int)l * ls;
     Cplx<T> o0, o1, o2, o3;
@@ -298,26 +306,24 @@ __device__ __forceinline__ void stockham_r4(const Cplx<T>* __restrict__ in, Cplx
 }
 
 // Radix-2 stage, one thread per butterfly.
-template <typename T, bool LINE_FAST>
+template <typename T, bool LINE_FAST, bool INV, int NL>
 __device__ __forceinline__ void stockham_r2(const Cplx<T>* __restrict__ in, Cplx<T>* __restrict__ out,
                                             int nl, int n, int ls, int es, int Ns,
-                                            const Cplx<T>* __restrict__ W, bool inverse, int tid, int nthr) {
+                                            const Cplx<T>* __restrict__ W, int tid, int nthr) {
   const int nb = n >> 1;
   const int total = nl * nb;
   const int scale = n / (Ns * 2);
   const FastDiv f_split = fast_div(LINE_FAST ? nl : nb), f_ns = fast_div(Ns);
   for (int idx = tid; idx < total; idx += nthr) {
-    const int qd = fdiv(idx, f_split);
-    const int rm = idx - qd * f_split.d;
-    const int l = LINE_FAST ? rm : qd;
-    const int j = LINE_FAST ? qd : rm;
+    int l, j;
+    split_item<LINE_FAST, NL>(idx, f_split, l, j);
     const int jq = fdiv(j, f_ns);
     const int k = j - jq * Ns;
     const Cplx<T>* src = in + (int)l * ls;
     Cplx<T> a = src[(int)j * es];
     Cplx<T> x = src[(int)(j + nb) * es];
     Cplx<T> w = W[scale * k];
-    T wy = inverse ? -w.y : w.y;
+    T wy = INV ? -w.y : w.y;
     Cplx<T> b;
     b.x = x.x * w.x - x.y * wy;
     b.y = x.x * wy + x.y * w.x;
@@ -335,24 +341,24 @@ __device__ __forceinline__ void stockham_r2(const Cplx<T>* __restrict__ in, Cplx
 // WARP: the calling threads are one warp (synchronised with __syncwarp),
 // otherwise the whole block (__syncthreads).  Returns the buffer holding the
 // result (a or b).
-template <typename T, bool LINE_FAST, bool WARP>
+template <typename T, bool LINE_FAST, bool WARP, bool INV, int NL = 0>
 __device__ __forceinline__ Cplx<T>* fft_run(const Radices& R, Cplx<T>* a, Cplx<T>* b, int nl, int n, int ls, int es,
-                                            const Cplx<T>* W, bool inverse, int tid, int nthr) {
+                                            const Cplx<T>* W, int tid, int nthr) {
   int Ns = 1;
   Cplx<T>* in = a;
   Cplx<T>* out = b;
   for (int s = 0; s < R.ns; ++s) {
     const int r = R.r[s];
     if (r == 4)
-      stockham_r4<T, LINE_FAST>(in, out, nl, n, ls, es, Ns, W, inverse, tid, nthr);
+      stockham_r4<T, LINE_FAST, INV, NL>(in, out, nl, n, ls, es, Ns, W, tid, nthr);
     else if (r == 2)
-      stockham_r2<T, LINE_FAST>(in, out, nl, n, ls, es, Ns, W, inverse, tid, nthr);
+      stockham_r2<T, LINE_FAST, INV, NL>(in, out, nl, n, ls, es, Ns, W, tid, nthr);
     else if (r == 3)
-      stockham_r35<T, LINE_FAST, 3>(in, out, nl, n, ls, es, Ns, W, inverse, tid, nthr);
+      stockham_r35<T, LINE_FAST, 3, INV, NL>(in, out, nl, n, ls, es, Ns, W, tid, nthr);
     else if (r == 5)
-      stockham_r35<T, LINE_FAST, 5>(in, out, nl, n, ls, es, Ns, W, inverse, tid, nthr);
+      stockham_r35<T, LINE_FAST, 5, INV, NL>(in, out, nl, n, ls, es, Ns, W, tid, nthr);
     else
-      stockham_odd<T, LINE_FAST, WARP>(in, out, nl, n, ls, es, Ns, r, W, inverse, tid, nthr);
+      stockham_odd<T, LINE_FAST, WARP, INV, NL>(in, out, nl, n, ls, es, Ns, r, W, tid, nthr);
     if (WARP)
       __syncwarp();
     else
@@ -370,20 +376,21 @@ __device__ __forceinline__ Cplx<T>* fft_run(const Radices& R, Cplx<T>* a, Cplx<T
 // Full transform by the whole block; returns the buffer holding the result (a or b).
 // Caller must __syncthreads() before (inputs written) -- this function
 // synchronises between stages and after the last one.
-template <typename T, bool LINE_FAST>
-__device__ Cplx<T>* fft_lines(Cplx<T>* a, Cplx<T>* b, int nl, int n, int ls, int es,
-                              const Cplx<T>* W, bool inverse) {
+// INV: inverse (unnormalised) transform.  NL > 0: nl == NL lines (a power of
+// two), known at compile time.
+template <typename T, bool LINE_FAST, bool INV, int NL = 0>
+__device__ Cplx<T>* fft_lines(Cplx<T>* a, Cplx<T>* b, int nl, int n, int ls, int es, const Cplx<T>* W) {
   Radices R;
   factor_radices(n, R);
-  return fft_run<T, LINE_FAST, false>(R, a, b, nl, n, ls, es, W, inverse, threadIdx.x, blockDim.x);
+  return fft_run<T, LINE_FAST, false, INV, NL>(R, a, b, nl, n, ls, es, W, threadIdx.x, blockDim.x);
 }
 
 // One contiguous line of length n transformed by one warp (lane = 0..31),
 // ping-ponging between a and b; the caller __syncwarp()s after writing a.
-template <typename T>
+template <typename T, bool INV>
 __device__ __forceinline__ Cplx<T>* warp_fft(const Radices& R, Cplx<T>* a, Cplx<T>* b, int n, const Cplx<T>* W,
-                                             bool inverse, int lane) {
-  return fft_run<T, false, true>(R, a, b, 1, n, n, 1, W, inverse, lane, 32);
+                                             int lane) {
+  return fft_run<T, false, true, INV>(R, a, b, 1, n, n, 1, W, lane, 32);
 }
 
 }  // namespace admp

@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(256) fft_z_fwd_kernel(Batch b, const T* __rest
     A[p * K2 + t] = z;
   }
   __syncthreads();
-  Cplx<T>* R = fft_lines<T, false>(A, B, np, K2, K2, 1, W, false);
+  Cplx<T>* R = fft_lines<T, false, false>(A, B, np, K2, K2, 1, W);
   Cplx<T>* H = spec + d.spec_off;
   for (int idx = threadIdx.x; idx < np * K2h; idx += blockDim.x) {
     const int p = fdiv(idx, fdK2h), k = idx - p * K2h;
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(256) fft_y_kernel(Batch b, Cplx<T>* __restrict
     A[y * zb + c] = H[(size_t)y * K2h + c];
   }
   __syncthreads();
-  Cplx<T>* R = fft_lines<T, true>(A, B, nz, K1, 1, zb, W, INV);
+  Cplx<T>* R = fft_lines<T, true, INV>(A, B, nz, K1, 1, zb, W);
   for (int idx = threadIdx.x; idx < K1 * nz; idx += blockDim.x) {
     const int y = fdiv(idx, fdnz), c = idx - y * nz;
     H[(size_t)y * K2h + c] = R[y * zb + c];
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
     A[x * zb + c] = H[(size_t)x * xs + c];
   }
   __syncthreads();
-  Cplx<T>* R = fft_lines<T, true>(A, B, nz, K0, 1, zb, W, false);
+  Cplx<T>* R = fft_lines<T, true, false>(A, B, nz, K0, 1, zb, W);
   Cplx<T>* F = (R == A) ? B : A;
   const double kappa = d.kappa;
   const double inv4k2 = 1.0 / (4.0 * kappa * kappa);
@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
     R[x * zb + c] = S;
   }
   block_atomic_sum<10>(v, acc + (size_t)s * kAccStride + kAccErec, red);
-  Cplx<T>* P = fft_lines<T, true>(R, F, nz, K0, 1, zb, W, true);
+  Cplx<T>* P = fft_lines<T, true, true>(R, F, nz, K0, 1, zb, W);
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
     const int x = fdiv(idx, fdnz), c = idx - x * nz;
     H[(size_t)x * xs + c] = P[x * zb + c];
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __r
     A[idx] = z;
   }
   __syncthreads();
-  Cplx<T>* R = fft_lines<T, false>(A, B, nzl, K2, K2, 1, W2, false);
+  Cplx<T>* R = fft_lines<T, false, false>(A, B, nzl, K2, K2, 1, W2);
   Cplx<T>* U = (R == A) ? B : A;
   // unpack the two-for-one transforms into U[y][pl][kz]
   const int ys = npl * K2h;  // element stride of the y lines
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __r
     if (2 * p + 1 < K1) U[(2 * p + 1) * ys + pl * K2h + k] = c;
   }
   __syncthreads();
-  Cplx<T>* V = fft_lines<T, true>(U, R, npl * K2h, K1, 1, ys, W1, false);
+  Cplx<T>* V = fft_lines<T, true, false>(U, R, npl * K2h, K1, 1, ys, W1);
   Cplx<T>* H = spec + d.spec_off + (size_t)x0 * K1 * K2h;
   for (int idx = threadIdx.x; idx < npl * K1 * K2h; idx += blockDim.x) {
     const int pl = fdiv(idx, fdP), rem = idx - pl * (K1 * K2h);
@@ -554,7 +554,7 @@ __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T
     A[y * ys + pl * K2h + kz] = H[idx];
   }
   __syncthreads();
-  Cplx<T>* V = fft_lines<T, true>(A, B, npl * K2h, K1, 1, ys, W1, true);
+  Cplx<T>* V = fft_lines<T, true, true>(A, B, npl * K2h, K1, 1, ys, W1);
   Cplx<T>* Z = (V == A) ? B : A;
   const int nzl = npl * np;
   for (int idx = threadIdx.x; idx < nzl * K2; idx += blockDim.x) {
@@ -580,7 +580,7 @@ __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T
     Z[idx] = z;
   }
   __syncthreads();
-  Cplx<T>* R = fft_lines<T, false>(Z, V, nzl, K2, K2, 1, W2, true);
+  Cplx<T>* R = fft_lines<T, false, true>(Z, V, nzl, K2, K2, 1, W2);
   T* M = mesh + d.mesh_off + (size_t)x0 * K1 * K2;
   for (int idx = threadIdx.x; idx < nzl * K2; idx += blockDim.x) {
     const int line = fdiv(idx, fdK2), t = idx - line * K2;
@@ -657,7 +657,7 @@ __global__ void __launch_bounds__(256) fft_x_apply_kernel(Batch b, Cplx<T>* __re
     A[x * zb + c] = H[(size_t)x * xs + c];
   }
   __syncthreads();
-  Cplx<T>* R = fft_lines<T, true>(A, B, nz, K0, 1, zb, W, false);
+  Cplx<T>* R = fft_lines<T, true, false>(A, B, nz, K0, 1, zb, W);
   Cplx<T>* F = (R == A) ? B : A;
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
     const int x = fdiv(idx, fdnz), c = idx - x * nz;
@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(256) fft_x_apply_kernel(Batch b, Cplx<T>* __re
     R[x * zb + c] = v;
   }
   __syncthreads();
-  Cplx<T>* P = fft_lines<T, true>(R, F, nz, K0, 1, zb, W, true);
+  Cplx<T>* P = fft_lines<T, true, true>(R, F, nz, K0, 1, zb, W);
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
     const int x = fdiv(idx, fdnz), c = idx - x * nz;
     H[(size_t)x * xs + c] = P[x * zb + c];
@@ -717,7 +717,7 @@ __global__ void __launch_bounds__(256) fft_z_inv_kernel(Batch b, const Cplx<T>* 
     A[p * K2 + t] = z;
   }
   __syncthreads();
-  Cplx<T>* R = fft_lines<T, false>(A, B, np, K2, K2, 1, W, true);
+  Cplx<T>* R = fft_lines<T, false, true>(A, B, np, K2, K2, 1, W);
   T* M = mesh + d.mesh_off;
   for (int idx = threadIdx.x; idx < np * K2; idx += blockDim.x) {
     const int p = fdiv(idx, fdK2), t = idx - p * K2;

@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(kClusterThreads, 2)
       wa[t] = z;
     }
     __syncwarp();
-    const Cplx<T>* Z = warp_fft<T>(R2, wa, wb, K2, W2, false, lane);
+    const Cplx<T>* Z = warp_fft<T, false>(R2, wa, wb, K2, W2, lane);
     for (int k = lane; k < K2h; k += 32) {
       const Cplx<T> a = Z[k], m = Z[k == 0 ? 0 : K2 - k];
       Cplx<T> u, c;
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(kClusterThreads, 2)
     Cplx<T>* col = planes + (size_t)lp * PS + kz;
     for (int y = lane; y < K1; y += 32) wa[y] = col[(size_t)y * RS];
     __syncwarp();
-    const Cplx<T>* Y = warp_fft<T>(R1, wa, wb, K1, W1, false, lane);
+    const Cplx<T>* Y = warp_fft<T, false>(R1, wa, wb, K1, W1, lane);
     for (int y = lane; y < K1; y += 32) col[(size_t)y * RS] = Y[y];
     __syncwarp();
   }
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kClusterThreads, 2)
         wa[x] = rbase[owner][(size_t)(x - owner * P) * PS + off];
       }
       __syncwarp();
-      Cplx<T>* X = warp_fft<T>(R0, wa, wb, K0, W0, false, lane);
+      Cplx<T>* X = warp_fft<T, false>(R0, wa, wb, K0, W0, lane);
       for (int x = lane; x < K0; x += 32) {
         const T gm = G[(size_t)x * gxs + c];
         X[x].x *= gm;
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(kClusterThreads, 2)
       }
       __syncwarp();
       Cplx<T>* F = X == wa ? wb : wa;
-      const Cplx<T>* Q = warp_fft<T>(R0, X, F, K0, W0, true, lane);
+      const Cplx<T>* Q = warp_fft<T, true>(R0, X, F, K0, W0, lane);
       for (int x = lane; x < K0; x += 32) {
         const int owner = x / P;
         rbase[owner][(size_t)(x - owner * P) * PS + off] = Q[x];
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(kClusterThreads, 2)
     Cplx<T>* col = planes + (size_t)lp * PS + kz;
     for (int y = lane; y < K1; y += 32) wa[y] = col[(size_t)y * RS];
     __syncwarp();
-    const Cplx<T>* Y = warp_fft<T>(R1, wa, wb, K1, W1, true, lane);
+    const Cplx<T>* Y = warp_fft<T, true>(R1, wa, wb, K1, W1, lane);
     for (int y = lane; y < K1; y += 32) col[(size_t)y * RS] = Y[y];
     __syncwarp();
   }
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(kClusterThreads, 2)
       wa[t] = z;
     }
     __syncwarp();
-    const Cplx<T>* Z = warp_fft<T>(R2, wa, wb, K2, W2, true, lane);
+    const Cplx<T>* Z = warp_fft<T, true>(R2, wa, wb, K2, W2, lane);
     T* f0 = reinterpret_cast<T*>(r0);
     T* f1 = reinterpret_cast<T*>(r1);
     for (int t = lane; t < K2; t += 32) {

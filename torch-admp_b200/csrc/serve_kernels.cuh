@@ -492,42 +492,59 @@ static __global__ void __launch_bounds__(256)
       const long long st = pstart[i];
       const int n = pcnt[i];
       T g0 = 0, g1 = 0, g2 = 0, e = 0;
-      for (int k = lane; k < n; k += 32) {
-        const int j = col[st + k];
-        T dr[3];
-        if (frac64) {
-          // displacement from double coordinates: close pairs keep full relative precision
-          double d64[3];
-          disp(fi64, frac64[j], bx, d64);
-          dr[0] = (T)d64[0];
-          dr[1] = (T)d64[1];
-          dr[2] = (T)d64[2];
-        } else {
-          disp(fi, frac[j], bx, dr);
+      // three entries per lane per trip, their loads issued before any is used
+      for (int k0 = 0; k0 < n; k0 += 96) {
+        int jj[3];
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+          const int k = k0 + lane + 32 * u;
+          jj[u] = k < n ? col[st + k] : -1;
         }
-        const T r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
-        const T r = sqrt_t(r2);
-        const T inv = T(1) / r;
-        const T qq = qi * q[j] * kt;
-        const T x = kappa * r;
-        const T er = erfc_t(x);
-        T ep = er * inv;
-        T dd = -tsp * kappa * exp_t(-x * x) * inv - er * inv * inv;
-        if (damp) {
-          const T ej = eta[j];
-          T eij = sqrt_t((ei * ei + ej * ej) * T(0.5));
-          if (eij == T(0)) eij = T(1e-10);
-          const T y = r / (T(2) * eij);
-          const T ed = erfc_t(y);
-          ep -= ed * inv;
-          dd += tsp * exp_t(-y * y) / (T(2) * eij) * inv + ed * inv * inv;
+        T drr[3][3], qjj[3], ejj[3];
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+          const int j = jj[u] >= 0 ? jj[u] : i;
+          if (frac64) {
+            // displacement from double coordinates: close pairs keep full relative precision
+            double d64[3];
+            disp(fi64, frac64[j], bx, d64);
+            drr[u][0] = (T)d64[0];
+            drr[u][1] = (T)d64[1];
+            drr[u][2] = (T)d64[2];
+          } else {
+            disp(fi, frac[j], bx, drr[u]);
+          }
+          qjj[u] = q[j];
+          ejj[u] = damp ? eta[j] : T(0);
         }
-        e += qq * ep;
-        // dE/dr_i = dE/dr * d r / d r_i = dd * qq * (-(r_j - r_i) / r)
-        const T gs = -dd * qq * inv;
-        g0 += gs * dr[0];
-        g1 += gs * dr[1];
-        g2 += gs * dr[2];
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+          if (jj[u] < 0) continue;
+          const T* dr = drr[u];
+          const T r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+          const T r = sqrt_t(r2);
+          const T inv = T(1) / r;
+          const T qq = qi * qjj[u] * kt;
+          const T x = kappa * r;
+          const T er = erfc_t(x);
+          T ep = er * inv;
+          T dd = -tsp * kappa * exp_t(-x * x) * inv - er * inv * inv;
+          if (damp) {
+            const T ej = ejj[u];
+            T eij = sqrt_t((ei * ei + ej * ej) * T(0.5));
+            if (eij == T(0)) eij = T(1e-10);
+            const T y = r / (T(2) * eij);
+            const T ed = erfc_t(y);
+            ep -= ed * inv;
+            dd += tsp * exp_t(-y * y) / (T(2) * eij) * inv + ed * inv * inv;
+          }
+          e += qq * ep;
+          // dE/dr_i = dE/dr * d r / d r_i = dd * qq * (-(r_j - r_i) / r)
+          const T gs = -dd * qq * inv;
+          g0 += gs * dr[0];
+          g1 += gs * dr[1];
+          g2 += gs * dr[2];
+        }
       }
       e = warp_sum(e);
       g0 = warp_sum(g0);

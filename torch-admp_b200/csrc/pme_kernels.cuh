@@ -74,6 +74,28 @@ __device__ __forceinline__ int find_sys(const Batch& b, int blk) {
 
 __device__ __forceinline__ int signed_k(int i, int K) { return i <= (K - 1) / 2 ? i : i - K; }
 
+// Block-strided loop over items [0, n) that issues U items' global loads
+// before using any of them: load(i) returns item i's value, use(i, v)
+// consumes it.  In a plain loop each trip's consumer (a shared-memory store)
+// waits for that trip's load, so a thread's loads would pay one memory
+// latency each, one after another.
+template <int U, typename V, typename L, typename S>
+__device__ __forceinline__ void block_batched(int n, L&& load, S&& use) {
+  for (int i0 = threadIdx.x; i0 < n; i0 += U * blockDim.x) {
+    V v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < n) v[u] = load(i);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < n) use(i, v[u]);
+    }
+  }
+}
+
 // Per-dimension B-spline structure factor used by the reference:
 // theta_d(n) = sum_{m=-2..2} M6(m+3) cos(2 pi m n / K)   (pme.py:412-432)
 __device__ __forceinline__ double theta_1d(int n, int K) {
@@ -379,10 +401,16 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
   }
   Cplx<T>* H = spec + d.spec_off + c0;
   const size_t xs = (size_t)K1 * K2h;
-  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = fdiv(idx, fdnz), c = idx - x * nz;
-    A[x * zb + c] = H[(size_t)x * xs + c];
-  }
+  block_batched<4, Cplx<T>>(
+      K0 * nz,
+      [&](int idx) {
+        const int x = fdiv(idx, fdnz), c = idx - x * nz;
+        return H[(size_t)x * xs + c];
+      },
+      [&](int idx, const Cplx<T>& v) {
+        const int x = fdiv(idx, fdnz), c = idx - x * nz;
+        A[x * zb + c] = v;
+      });
   __syncthreads();
   Cplx<T>* R = fft_lines<T, true, false>(A, B, nz, K0, 1, zb, W);
   Cplx<T>* F = (R == A) ? B : A;
@@ -491,15 +519,18 @@ __global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __r
   make_twiddles(W2, K2);
   const T* Q = mesh + d.mesh_off + (size_t)x0 * K1 * K2;
   const int nzl = npl * np;  // z line pairs of the block
-  for (int idx = threadIdx.x; idx < nzl * K2; idx += blockDim.x) {
-    const int line = fdiv(idx, fdK2), t = idx - line * K2;
-    const int pl = fdiv(line, fdnp), p = line - pl * np;
-    const T* Qp = Q + (size_t)pl * K1 * K2;
-    Cplx<T> z;
-    z.x = Qp[(size_t)(2 * p) * K2 + t];
-    z.y = 2 * p + 1 < K1 ? Qp[(size_t)(2 * p + 1) * K2 + t] : T(0);
-    A[idx] = z;
-  }
+  block_batched<4, Cplx<T>>(
+      nzl * K2,
+      [&](int idx) {
+        const int line = fdiv(idx, fdK2), t = idx - line * K2;
+        const int pl = fdiv(line, fdnp), p = line - pl * np;
+        const T* Qp = Q + (size_t)pl * K1 * K2;
+        Cplx<T> z;
+        z.x = Qp[(size_t)(2 * p) * K2 + t];
+        z.y = 2 * p + 1 < K1 ? Qp[(size_t)(2 * p + 1) * K2 + t] : T(0);
+        return z;
+      },
+      [&](int idx, const Cplx<T>& z) { A[idx] = z; });
   __syncthreads();
   Cplx<T>* R = fft_lines<T, false, false>(A, B, nzl, K2, K2, 1, W2);
   Cplx<T>* U = (R == A) ? B : A;
@@ -548,11 +579,13 @@ __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T
   make_twiddles(W2, K2);
   const int ys = npl * K2h;
   const Cplx<T>* H = spec + d.spec_off + (size_t)x0 * K1 * K2h;
-  for (int idx = threadIdx.x; idx < npl * K1 * K2h; idx += blockDim.x) {
-    const int pl = fdiv(idx, fdP), rem = idx - pl * (K1 * K2h);
-    const int y = fdiv(rem, fdK2h), kz = rem - y * K2h;
-    A[y * ys + pl * K2h + kz] = H[idx];
-  }
+  block_batched<4, Cplx<T>>(
+      npl * K1 * K2h, [&](int idx) { return H[idx]; },
+      [&](int idx, const Cplx<T>& v) {
+        const int pl = fdiv(idx, fdP), rem = idx - pl * (K1 * K2h);
+        const int y = fdiv(rem, fdK2h), kz = rem - y * K2h;
+        A[y * ys + pl * K2h + kz] = v;
+      });
   __syncthreads();
   Cplx<T>* V = fft_lines<T, true, true>(A, B, npl * K2h, K1, 1, ys, W1);
   Cplx<T>* Z = (V == A) ? B : A;
@@ -652,21 +685,32 @@ __global__ void __launch_bounds__(256) fft_x_apply_kernel(Batch b, Cplx<T>* __re
   Cplx<T>* H = spec + d.spec_off + c0;
   const T* G = green + d.green_off + c0;
   const size_t xs = (size_t)K1 * K2h;
-  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = fdiv(idx, fdnz), c = idx - x * nz;
-    A[x * zb + c] = H[(size_t)x * xs + c];
-  }
+  block_batched<4, Cplx<T>>(
+      K0 * nz,
+      [&](int idx) {
+        const int x = fdiv(idx, fdnz), c = idx - x * nz;
+        return H[(size_t)x * xs + c];
+      },
+      [&](int idx, const Cplx<T>& v) {
+        const int x = fdiv(idx, fdnz), c = idx - x * nz;
+        A[x * zb + c] = v;
+      });
   __syncthreads();
   Cplx<T>* R = fft_lines<T, true, false>(A, B, nz, K0, 1, zb, W);
   Cplx<T>* F = (R == A) ? B : A;
-  for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {
-    const int x = fdiv(idx, fdnz), c = idx - x * nz;
-    const T gm = G[(size_t)x * xs + c];
-    Cplx<T> v = R[x * zb + c];
-    v.x *= gm;
-    v.y *= gm;
-    R[x * zb + c] = v;
-  }
+  block_batched<4, T>(
+      K0 * nz,
+      [&](int idx) {
+        const int x = fdiv(idx, fdnz), c = idx - x * nz;
+        return G[(size_t)x * xs + c];
+      },
+      [&](int idx, T gm) {
+        const int x = fdiv(idx, fdnz), c = idx - x * nz;
+        Cplx<T> v = R[x * zb + c];
+        v.x *= gm;
+        v.y *= gm;
+        R[x * zb + c] = v;
+      });
   __syncthreads();
   Cplx<T>* P = fft_lines<T, true, true>(R, F, nz, K0, 1, zb, W);
   for (int idx = threadIdx.x; idx < K0 * nz; idx += blockDim.x) {

@@ -810,30 +810,45 @@ __global__ void __launch_bounds__(256) gather_kernel(Batch b, const T* __restric
     T my_pot = 0, my_g0 = 0, my_g1 = 0, my_g2 = 0;
     for (int j0 = 0; j0 < na; j0 += 8) {
       const int j1 = min(j0 + 8, na);
-      for (int j = j0; j < j1; ++j) {
-        const T* w = ws.w + j * 18;
-        const int* ox = ws.ox + j * 6;
-        const T wy = w[6 + y0], wz = w[12 + z0];
-        const int oyz = wrap_up(ws.byz[2 * j] + y0, d.K1) * d.K2 + wrap_up(ws.byz[2 * j + 1] + z0, d.K2);
-        T sw = 0, sdw = 0;
+      // GU atoms at a time: their 6 GU mesh loads are issued before the first reduction
+      constexpr int GU = sizeof(T) == 8 ? 2 : 4;
+      for (int jb = j0; jb < j1; jb += GU) {
+        T fm[GU][6];
 #pragma unroll
-        for (int dx = 0; dx < 6; ++dx) {
-          const T f = M[ox[dx] + oyz];
-          sw += f * w[dx];
-          if (FORCES) sdw += f * ws.dw[j * 18 + dx];
+        for (int u = 0; u < GU; ++u) {
+          const int j = jb + u;
+          if (j < j1) {
+            const int* ox = ws.ox + j * 6;
+            const int oyz = wrap_up(ws.byz[2 * j] + y0, d.K1) * d.K2 + wrap_up(ws.byz[2 * j + 1] + z0, d.K2);
+#pragma unroll
+            for (int dx = 0; dx < 6; ++dx) fm[u][dx] = M[ox[dx] + oyz];
+          }
         }
-        T pot = sw * wy * wz, g0 = 0, g1 = 0, g2 = 0;
-        pot = warp_sum(pot);
-        if (FORCES) {
-          g0 = warp_sum(sdw * wy * wz);
-          g1 = warp_sum(sw * ws.dw[j * 18 + 6 + y0] * wz);
-          g2 = warp_sum(sw * wy * ws.dw[j * 18 + 12 + z0]);
-        }
-        if (lane == j) {
-          my_pot = pot;
-          my_g0 = g0;
-          my_g1 = g1;
-          my_g2 = g2;
+#pragma unroll
+        for (int u = 0; u < GU; ++u) {
+          const int j = jb + u;
+          if (j >= j1) break;
+          const T* w = ws.w + j * 18;
+          const T wy = w[6 + y0], wz = w[12 + z0];
+          T sw = 0, sdw = 0;
+#pragma unroll
+          for (int dx = 0; dx < 6; ++dx) {
+            sw += fm[u][dx] * w[dx];
+            if (FORCES) sdw += fm[u][dx] * ws.dw[j * 18 + dx];
+          }
+          T pot = sw * wy * wz, g0 = 0, g1 = 0, g2 = 0;
+          pot = warp_sum(pot);
+          if (FORCES) {
+            g0 = warp_sum(sdw * wy * wz);
+            g1 = warp_sum(sw * ws.dw[j * 18 + 6 + y0] * wz);
+            g2 = warp_sum(sw * wy * ws.dw[j * 18 + 12 + z0]);
+          }
+          if (lane == j) {
+            my_pot = pot;
+            my_g0 = g0;
+            my_g1 = g1;
+            my_g2 = g2;
+          }
         }
       }
       // the last four columns of atoms j0 .. j1-1, reduced over each atom's four lanes

@@ -617,13 +617,24 @@ static __global__ void __launch_bounds__(256)
   const int grp = threadIdx.x / kSpmvLanes, ngrp = blockDim.x / kSpmvLanes;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
-  // every lane runs the same number of loop trips (shuffles below use the full mask)
+  // every lane runs the same number of loop trips (shuffles below use the full mask);
+  // the next trip's row start and length are loaded while this trip's row is summed
+  long long st_next = 0;
+  int n_next = 0;
+  if (a0 + grp < a1) {
+    st_next = pstart[d.atom_off + a0 + grp];
+    n_next = pcnt[d.atom_off + a0 + grp];
+  }
   for (int base = a0; base < a1; base += ngrp) {
     const int a = base + grp;
     const bool row = a < a1;
     const int i = d.atom_off + (row ? a : a0);
-    const long long st = pstart[i];
-    const int n = row ? pcnt[i] : 0;
+    const long long st = st_next;
+    const int n = row ? n_next : 0;
+    if (a + ngrp < a1) {
+      st_next = pstart[i + ngrp];
+      n_next = pcnt[i + ngrp];
+    }
     T acc = 0;
     for (int k0 = 0; k0 < n; k0 += kSpmvLanes * kSpmvUnroll) {
       int c[kSpmvUnroll];

@@ -134,10 +134,14 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
     __syncwarp();
   else
     __syncthreads();
-  const int total2 = (h + 1) * total1;
+  // step 2 items: class 0 forms X_0, class c >= 1 the output pairs
+  // kk = 1 + QK (c - 1) .. QK c, which share each load of s_t and d_t
+  constexpr int QK = 2;
+  const int nq = (h + QK - 1) / QK;
+  const int total2 = (nq + 1) * total1;
   for (int idx = tid; idx < total2; idx += nthr) {
-    const int kk = fdiv(idx, f_items);
-    const int it = idx - kk * f_items.d;
+    const int c = fdiv(idx, f_items);
+    const int it = idx - c * f_items.d;
     int l, j;
     split_item<LINE_FAST, NL>(it, f_split, l, j);
     const int jq = fdiv(j, f_ns);
@@ -146,8 +150,8 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
     Cplx<T>* dst = in + (int)l * ls;
     const int base = jq * Ns * r + k;
     const Cplx<T> v0 = src[(int)base * es];
-    T ax = v0.x, ay = v0.y;
-    if (kk == 0) {
+    if (c == 0) {
+      T ax = v0.x, ay = v0.y;
       for (int u = 1; u <= h; ++u) {
         const Cplx<T> sv = src[(int)(base + u * Ns) * es];
         ax += sv.x;
@@ -159,28 +163,46 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
       dst[(int)base * es] = X;
       continue;
     }
-    T bx = 0, by = 0;
-    int e = 0;
+    const int kk0 = 1 + (c - 1) * QK;
+    T ax[QK], ay[QK], bx[QK], by[QK];
+    int e[QK], kq[QK];
+#pragma unroll
+    for (int t = 0; t < QK; ++t) {
+      kq[t] = min(kk0 + t, h);  // past h: computed, not stored
+      e[t] = 0;
+      ax[t] = v0.x;
+      ay[t] = v0.y;
+      bx[t] = T(0);
+      by[t] = T(0);
+    }
     for (int u = 1; u <= h; ++u) {
-      e += kk;
-      if (e >= r) e -= r;
-      const Cplx<T> w = W[e * wr];  // (cos, -sin) of 2 pi e / r
       const Cplx<T> sv = src[(int)(base + u * Ns) * es];
       const Cplx<T> dv = src[(int)(base + (h + u) * Ns) * es];
-      ax += sv.x * w.x;
-      ay += sv.y * w.x;
-      bx -= dv.x * w.y;
-      by -= dv.y * w.y;
+#pragma unroll
+      for (int t = 0; t < QK; ++t) {
+        e[t] += kq[t];
+        if (e[t] >= r) e[t] -= r;
+        const Cplx<T> w = W[e[t] * wr];  // (cos, -sin) of 2 pi e / r
+        ax[t] += sv.x * w.x;
+        ay[t] += sv.y * w.x;
+        bx[t] -= dv.x * w.y;
+        by[t] -= dv.y * w.y;
+      }
     }
-    // forward: X_k = A - i B, X_{r-k} = A + i B (inverse: signs swapped); -i B = (B.y, -B.x)
-    const T ibx = INV ? -by : by, iby = INV ? bx : -bx;
-    Cplx<T> X1, X2;
-    X1.x = ax + ibx;
-    X1.y = ay + iby;
-    X2.x = ax - ibx;
-    X2.y = ay - iby;
-    dst[(int)(base + kk * Ns) * es] = X1;
-    dst[(int)(base + (r - kk) * Ns) * es] = X2;
+#pragma unroll
+    for (int t = 0; t < QK; ++t) {
+      const int kk = kk0 + t;
+      if (kk > h) break;
+      // forward: X_k = A - i B, X_{r-k} = A + i B (inverse: signs swapped); -i B = (B.y, -B.x)
+      const T ibx = INV ? -by[t] : by[t], iby = INV ? bx[t] : -bx[t];
+      Cplx<T> X1, X2;
+      X1.x = ax[t] + ibx;
+      X1.y = ay[t] + iby;
+      X2.x = ax[t] - ibx;
+      X2.y = ay[t] - iby;
+      dst[(int)(base + kk * Ns) * es] = X1;
+      dst[(int)(base + (r - kk) * Ns) * es] = X2;
+    }
   }
 }
 

@@ -325,6 +325,89 @@ static int launch_cluster_pot(const ClusterPlan& cp, const RecipPlan<T>& rp, con
   return ADMP_OK;
 }
 
+// CSR SpMV (as csr_spmv_kernel) fused with the end of the matvec (as
+// qeq_finish_kernel): per row h = (recip + J_real v)_i + diag_i v_i + nn sum(v)
+// (+ slab terms), Hv_i = h, and the block sums of v.h and C.h into the CG
+// scalars -- one pass over the rows instead of two.
+template <typename T>
+static __global__ void __launch_bounds__(256)
+    csr_spmv_finish_kernel(Batch b, QEqParams prm, const long long* __restrict__ pstart, const int* __restrict__ pcnt,
+                           const int* __restrict__ col, const T* __restrict__ coef, const T* __restrict__ v,
+                           T* __restrict__ Hv, const double* __restrict__ diag, const double* __restrict__ zc,
+                           CGScal* __restrict__ sc, double* __restrict__ hv_out) {
+  __shared__ double red[5 * 32];
+  const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
+  const SysDesc& d = b.s[s0];
+  const int s = d.box_idx;
+  if (sc[s].done) return;
+  const CGScal& S = sc[s];
+  const double sp = S.sp, spz = S.spz, spz2 = S.spz2;
+  const bool slab = (prm.flags & ADMP_QEQ_SLAB) != 0;
+  const int nc = S.n_const;
+  double accs[5] = {0, 0, 0, 0, 0};
+  const int sub = threadIdx.x & (kSpmvLanes - 1);
+  const int grp = threadIdx.x / kSpmvLanes, ngrp = blockDim.x / kSpmvLanes;
+  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
+  const int a1 = min(a0 + b.apb, d.natoms);
+  long long st_next = 0;
+  int n_next = 0;
+  if (a0 + grp < a1) {
+    st_next = pstart[d.atom_off + a0 + grp];
+    n_next = pcnt[d.atom_off + a0 + grp];
+  }
+  for (int base = a0; base < a1; base += ngrp) {
+    const int a = base + grp;
+    const bool row = a < a1;
+    const int i = d.atom_off + (row ? a : a0);
+    const long long st = st_next;
+    const int n = row ? n_next : 0;
+    if (a + ngrp < a1) {
+      st_next = pstart[i + ngrp];
+      n_next = pcnt[i + ngrp];
+    }
+    T acc = 0;
+    for (int k0 = 0; k0 < n; k0 += kSpmvLanes * kSpmvUnroll) {
+      int c[kSpmvUnroll];
+      T w[kSpmvUnroll];
+#pragma unroll
+      for (int u = 0; u < kSpmvUnroll; ++u) {
+        const int k = k0 + sub + u * kSpmvLanes;
+        const bool ok = k < n;
+        c[u] = ok ? col[st + k] : -1;
+        w[u] = ok ? coef[st + k] : T(0);
+      }
+      T vv[kSpmvUnroll];
+#pragma unroll
+      for (int u = 0; u < kSpmvUnroll; ++u) vv[u] = c[u] >= 0 ? v[c[u]] : T(0);
+#pragma unroll
+      for (int u = 0; u < kSpmvUnroll; ++u) acc += w[u] * vv[u];
+    }
+#pragma unroll
+    for (int o = kSpmvLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (row && sub == 0) {
+      const T hv = Hv[i] + acc;
+      const double x = (double)v[i];
+      double h = (double)hv + diag[i] * x + S.nn * sp;
+      if (slab) {
+        const double z = zc[i];
+        h += S.pre * (2.0 * z * spz - spz2 - z * z * sp - S.Lz2 / 6.0 * sp);
+      }
+      Hv[i] = (T)h;
+      if (hv_out) hv_out[i] = h;
+      accs[0] += x * h;
+#pragma unroll
+      for (int cc = 0; cc < kMaxConst; ++cc)  // serving constraints are total-charge rows
+        if (cc < nc) accs[1 + cc] += h;
+    }
+  }
+  double a1v[1] = {accs[0]};
+  block_atomic_sum<1>(a1v, &sc[s].pHp, red);
+  if (nc > 0) {
+    double a4[4] = {accs[1], accs[2], accs[3], accs[4]};
+    block_atomic_sum<4>(a4, sc[s].Cv, red);
+  }
+}
+
 // H v for the listed systems: Hv must be zeroed, sums of v in the CG state.
 template <typename T>
 static int srv_matvec(const admp_pools* P, const RecipPlan<T>& plan, QEqParams prm, const T* v, T* Hv,
@@ -335,12 +418,10 @@ static int srv_matvec(const admp_pools* P, const RecipPlan<T>& plan, QEqParams p
                                          (Cplx<T>*)P->spec, P->acc, ke, Hv, st, P->sorted, (const T*)P->green);
   if (s) return s;
   int h = prof_begin(st);
-  csr_spmv_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->pstart, P->pcnt, P->col, (const T*)P->coef, v, Hv, b.done,
-                                                  b.done_stride);
+  csr_spmv_finish_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, P->pstart, P->pcnt, P->col, (const T*)P->coef, v,
+                                                         Hv, P->cg_diag, P->cg_z, (CGScal*)P->cg_state, hv_out);
   prof_end(h, PK_CSR_SPMV, -1.0, st);
-  count_launches(2);
-  qeq_finish_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, v, Hv, P->cg_diag, P->cg_z, (const T*)nullptr, 0,
-                                                    (CGScal*)P->cg_state, hv_out);
+  count_launches(1);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
 }

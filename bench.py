@@ -52,7 +52,7 @@ LAT_RATE = 1000.0      # open-loop Poisson rate (requests/s) for the p50/p99 lat
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte, from one ncu capture of
 # the 400-request stream (x_apply 83.4 MB per launch, spread 58.4, gather 63.9); roofline.traffic = ratio x algorithmic bytes
 # per launch of this run, the launches of one chunk being alike in size at 400 and 2000 requests
-TRAFFIC_PER_ALG_BYTE = {"fft_x_green": 0.796, "spread": 1.216, "gather": 1.280}
+TRAFFIC_PER_ALG_BYTE = {"fft_x_green": 0.600, "spread": 0.959, "gather": 0.857}
 
 
 def parse():

@@ -50,8 +50,8 @@ RCUT, ETHRESH = 6.0, 5e-4
 TOL = 1e-7
 LAT_RATE = 1000.0      # open-loop Poisson rate (requests/s) for the p50/p99 latency pass
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte, from one ncu capture of
-# the 400-request stream (x_apply 83.4 MB per launch, spread 58.4, gather 63.9); roofline.traffic = ratio x algorithmic bytes
-# per launch of this run, the launches of one chunk being alike in size at 400 and 2000 requests
+# every launch of these kernels in five passes of the 400-request stream (x pass 85.5 MB per launch,
+# spread 62.5, gather 58.1); roofline.traffic = ratio x algorithmic bytes per launch of this run
 TRAFFIC_PER_ALG_BYTE = {"fft_x_green": 0.600, "spread": 0.959, "gather": 0.857}
 
 

@@ -22,6 +22,7 @@ All arithmetic runs in libadmp_b200.so (admp_serve_* entry points).
 """
 from __future__ import annotations
 
+import bisect
 import ctypes
 import math
 import time
@@ -105,16 +106,19 @@ class _Intervals:
         return None
 
     def release(self, off: int, n: int) -> None:
+        """Return [off, off + n) to the sorted free list, merged with its neighbours."""
         n = (n + self.align - 1) // self.align * self.align
-        self.free.append((off, off + n))
-        self.free.sort()
-        merged = []
-        for a, b in self.free:
-            if merged and merged[-1][1] == a:
-                merged[-1] = (merged[-1][0], b)
-            else:
-                merged.append((a, b))
-        self.free = merged
+        fr = self.free
+        a, b = off, off + n
+        k = bisect.bisect_left(fr, (a, b))
+        if k > 0 and fr[k - 1][1] == a:
+            k -= 1
+            a = fr[k][0]
+            del fr[k]
+        if k < len(fr) and fr[k][0] == b:
+            b = fr[k][1]
+            del fr[k]
+        fr.insert(k, (a, b))
 
     def used(self) -> int:
         return self.cap - sum(b - a for a, b in self.free)

@@ -116,11 +116,16 @@ __device__ __forceinline__ void stockham_odd(Cplx<T>* __restrict__ in, Cplx<T>* 
     for (int u = 1; u <= h; ++u) {
       const Cplx<T> a = src[(int)(j + u * nb) * es];
       const Cplx<T> c = src[(int)(j + (r - u) * nb) * es];
-      const Cplx<T> wa = W[scale * k * u];
-      const Cplx<T> wc = W[scale * k * (r - u)];
-      const T way = INV ? -wa.y : wa.y, wcy = INV ? -wc.y : wc.y;
-      const T ax = a.x * wa.x - a.y * way, ay = a.x * way + a.y * wa.x;
-      const T cx = c.x * wc.x - c.y * wcy, cy = c.x * wcy + c.y * wc.x;
+      T ax = a.x, ay = a.y, cx = c.x, cy = c.y;
+      if (Ns > 1) {  // the first stage's twiddles are all 1
+        const Cplx<T> wa = W[scale * k * u];
+        const Cplx<T> wc = W[scale * k * (r - u)];
+        const T way = INV ? -wa.y : wa.y, wcy = INV ? -wc.y : wc.y;
+        ax = a.x * wa.x - a.y * way;
+        ay = a.x * way + a.y * wa.x;
+        cx = c.x * wc.x - c.y * wcy;
+        cy = c.x * wcy + c.y * wc.x;
+      }
       Cplx<T> sv, dv;
       sv.x = ax + cx;
       sv.y = ay + cy;
@@ -228,8 +233,8 @@ __device__ __forceinline__ void stockham_r35(const Cplx<T>* __restrict__ in, Cpl
 #pragma unroll
     for (int t = 0; t < R; ++t) {
       const Cplx<T> x = src[(int)(j + t * nb) * es];
-      if (t == 0) {
-        v[0] = x;
+      if (t == 0 || Ns == 1) {  // first stage: every twiddle is 1
+        v[t] = x;
       } else {
         const Cplx<T> w = W[scale * k * t];
         const T wy = INV ? -w.y : w.y;
@@ -296,8 +301,8 @@ __device__ __forceinline__ void stockham_r4(const Cplx<T>* __restrict__ in, Cplx
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       Cplx<T> x = src[(int)(j + t * nb) * es];
-      if (t == 0) {
-        v[0] = x;
+      if (t == 0 || Ns == 1) {  // first stage: every twiddle is 1
+        v[t] = x;
       } else {
         Cplx<T> w = W[scale * k * t];
         T wy = INV ? -w.y : w.y;
@@ -344,11 +349,13 @@ __device__ __forceinline__ void stockham_r2(const Cplx<T>* __restrict__ in, Cplx
     const Cplx<T>* src = in + (int)l * ls;
     Cplx<T> a = src[(int)j * es];
     Cplx<T> x = src[(int)(j + nb) * es];
-    Cplx<T> w = W[scale * k];
-    T wy = INV ? -w.y : w.y;
-    Cplx<T> b;
-    b.x = x.x * w.x - x.y * wy;
-    b.y = x.x * wy + x.y * w.x;
+    Cplx<T> b = x;
+    if (Ns > 1) {  // the first stage's twiddles are all 1
+      const Cplx<T> w = W[scale * k];
+      const T wy = INV ? -w.y : w.y;
+      b.x = x.x * w.x - x.y * wy;
+      b.y = x.x * wy + x.y * w.x;
+    }
     const int base = jq * Ns * 2 + k;
     Cplx<T>* dst = out + (int)l * ls;
     Cplx<T> o0, o1;

@@ -158,3 +158,40 @@ def test_row_overflow_is_served_again(cuda, stream_and_oracle):
         assert out.status == 0
         assert abs(out.energy - E) / abs(E) < 1e-9
         assert np.abs(out.forces - F).max() / np.abs(F).max() < 1e-7
+
+
+def triclinic_requests():
+    """Requests in non-orthogonal cells: three cells per axis (the neighbour
+    search's fixed-image path) and two per axis (nearest-image path)."""
+    from admp_b200 import synthetic
+    from admp_b200.synthetic import Request
+    rng = np.random.default_rng(29)
+    out = []
+    for rid, box in enumerate([np.array([[20.0, 0.0, 0.0], [4.0, 19.0, 0.0], [-3.0, 2.5, 21.0]]),
+                               np.array([[13.0, 0.0, 0.0], [2.5, 12.8, 0.0], [1.0, -2.0, 13.5]])]):
+        n = int(abs(np.linalg.det(box)) * 0.1) // 2 * 2
+        pos = rng.random((n, 3)) @ box + rng.normal(0.0, 1.0, (n, 3))  # some atoms outside the cell
+        q = np.ones(n)
+        q[n // 2:] = -1.0
+        rng.shuffle(q)
+        out.append(Request(rid, "pme", 0.0, pos, box, charges=q))
+        # waters of a cubic cell mapped into the same cell by their fractional coordinates
+        L = 10.0
+        wpos, _, chi, hard, eta, _ = synthetic.water_system(max(8, n // 9), L, 40 + rid)
+        wpos = (wpos / L) @ box
+        out.append(Request(10 + rid, "qeq", 0.0, wpos, box, chi=chi, hardness=hard, eta=eta))
+    return out
+
+
+@pytest.mark.parametrize("dtype,etol,ftol,qtol", [(torch.float64, 1e-9, 1e-7, 1e-8), (torch.float32, 1e-5, 1e-4, 1e-5)])
+def test_serving_triclinic_cells_match_oracle(cuda, dtype, etol, ftol, qtol):
+    reqs = triclinic_requests()
+    refs = [oracle_result(r) for r in reqs]
+    res, _ = serve(reqs, dtype, 1e-10 if dtype == torch.float64 else 1e-7)
+    for r, (E, F, q) in zip(reqs, refs):
+        out = res[r.rid]
+        assert out.status == 0, (r.rid, out.status)
+        assert abs(out.energy - E) / abs(E) < etol, (r.rid, out.energy, E)
+        assert np.abs(out.forces - F).max() / np.abs(F).max() < ftol, r.rid
+        if q is not None:
+            assert np.abs(out.charges - q).max() < qtol, r.rid

@@ -179,7 +179,7 @@ class ClockSampler:
 
     def _read(self):
         for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+            self.lines.append((time.time(), ln.strip()))
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -189,10 +189,14 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, t0: float = None, t1: float = None):
+        """Samples taken in [t0, t1] (all of them when none falls there)."""
+        lines = [ln for t, ln in self.lines if t0 is None or t0 <= t <= t1]
+        if not lines:
+            lines = [ln for _, ln in self.lines]
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 7:
                 continue
@@ -324,6 +328,10 @@ def main():
         if world > 1:
             dist.barrier()
 
+    # the clock sampler (an nvidia-smi process) starts before the warm-up: its start-up attaches to the
+    # driver and would otherwise stall launches of the first timed pass; only its samples taken inside
+    # the timed region are summarised
+    clk = ClockSampler(dev.index).__enter__()
     # warm-up
     for _ in range(args.warmup):
         one_pass(dstream, to_host=False)
@@ -337,12 +345,14 @@ def main():
         eng.host_time[k] = 0.0
     barrier()
     torch.cuda.synchronize()
-    with ClockSampler(dev.index) as clk:
-        e0.record(st)
-        for _ in range(args.steps):
-            res = one_pass(dstream, to_host=False)
-        e1.record(st)
-        torch.cuda.synchronize()
+    t_clk0 = time.time()
+    e0.record(st)
+    for _ in range(args.steps):
+        res = one_pass(dstream, to_host=False)
+    e1.record(st)
+    torch.cuda.synchronize()
+    t_clk1 = time.time()
+    clk.__exit__()
     barrier()
     ms = e0.elapsed_time(e1)
     launches = L.launch_count() - launches0
@@ -424,7 +434,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample = cpu_baseline(stream, args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
-    clocks = clk.summary()
+    clocks = clk.summary(t_clk0, t_clk1)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -23,6 +23,7 @@ All arithmetic runs in libadmp_b200.so (admp_serve_* entry points).
 from __future__ import annotations
 
 import bisect
+import concurrent.futures
 import ctypes
 import math
 import time
@@ -62,6 +63,7 @@ class AdmpPools(ctypes.Structure):
 SERVE_CLUSTER_MATVEC = 1
 
 # ints per slot of the x-key tables (mesh planes along x + 1)
+_COPY_THREADS = 4  # host threads copying request arrays into the pinned staging buffers
 XKEY_STRIDE = 1024
 
 
@@ -241,6 +243,8 @@ class ServingEngine:
         self.results: List[Result] = []
         self.warm: Dict[object, np.ndarray] = {}
         self.stream = torch.cuda.current_stream(self.dev)
+        # worker threads for the host-side copies of request arrays into the pinned staging buffers
+        self._copy_pool = concurrent.futures.ThreadPoolExecutor(max_workers=_COPY_THREADS)
         self.pin = {}
         self.stats = {"ticks": 0, "launch_calls": 0, "admitted": 0, "h2d_bytes": 0, "d2h_bytes": 0, "retries": 0}
         self._fact_cache: Dict[int, tuple] = {}
@@ -458,14 +462,26 @@ class ServingEngine:
         npdt = {torch.float32: np.float32, torch.float64: np.float64}[dtype]
         n = dest.numel()
         host, th = self._stage_take(n, npdt)
+        jobs = []
         o = 0
         for a, p in zip(arrays, pads):
             v = np.asarray(a).reshape(-1)
-            host[o:o + v.size] = v
+            jobs.append((o, v))
             o += v.size
             if p:
                 host[o:o + p * width] = 0
                 o += p * width
+
+        def copy_part(k):
+            # numpy releases the GIL for these copies, so the parts run in parallel
+            for jo, jv in jobs[k::_COPY_THREADS]:
+                host[jo:jo + jv.size] = jv
+
+        if len(jobs) > 1 and n * host.itemsize >= (1 << 20):
+            list(self._copy_pool.map(copy_part, range(_COPY_THREADS)))
+        else:
+            for jo, jv in jobs:
+                host[jo:jo + jv.size] = jv
         dest.view(-1).copy_(th, non_blocking=True)
         return n * th.element_size()
 

@@ -151,3 +151,33 @@ def test_ewald_energy_with_cutoff_above_half_box(cuda):
     e2, f2 = run(9.0, lambda p, b, rc: nblist.dp_nblist(p, b, 4000, rc))
     assert abs(e2 - e1) / abs(e1) < 2e-6
     assert rel(f2, f1) < 2e-5
+
+
+def test_vesin_half_list_with_self_images(cuda):
+    """rc above the box length: vesin_nblist keeps one of each +-n self-image
+    couple with scale 1, dp_nblist both with scale 1/2; their pair energies agree."""
+    from admp_b200 import nblist
+    from admp_b200.ops import image_neighbor_pairs
+    rng = np.random.default_rng(13)
+    box = np.array([[7.0, 0.0, 0.0], [1.0, 7.5, 0.0], [0.5, -0.5, 8.0]])
+    pos = rng.random((30, 3)) @ box
+    rc = 9.0
+    p_dp, ds_dp, bs_dp = nblist.dp_nblist(T(pos, cuda), T(box, cuda), 10000, rc)
+    p_v, ds_v, bs_v = nblist.vesin_nblist(T(pos, cuda), T(box, cuda), rc)
+    pr, sh, n_ij, _ = image_neighbor_pairs(T(pos, cuda), T(box, cuda), rc, -1)
+    n_self = pr.shape[0] - n_ij
+    assert n_self > 0 and n_self % 2 == 0
+    assert p_v.shape[0] == n_ij + n_self // 2 and bool((bs_v == 1).all())
+    # kept self images: first non-zero shift component positive
+    s = sh[n_ij:].cpu().numpy()
+    first = np.where(s[:, 0] != 0, s[:, 0], np.where(s[:, 1] != 0, s[:, 1], s[:, 2]))
+    assert (first > 0).sum() == n_self // 2
+    # any pair function summed with the buffer scales is the same over both lists
+    q = rng.normal(size=30)
+    qt = T(q, cuda)
+
+    def pair_sum(p, ds, bs):
+        return float((qt[p[:, 0]] * qt[p[:, 1]] * torch.erfc(0.3 * ds) / ds * bs.to(ds.dtype)).sum())
+
+    a, b = pair_sum(p_dp, ds_dp, bs_dp), pair_sum(p_v, ds_v, bs_v)
+    assert abs(a - b) <= 1e-12 * max(1.0, abs(a))

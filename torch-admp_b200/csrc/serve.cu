@@ -325,7 +325,7 @@ static int launch_cluster_pot(const ClusterPlan& cp, const RecipPlan<T>& rp, con
   return ADMP_OK;
 }
 
-// CSR SpMV (as csr_spmv_kernel) fused with the end of the matvec (as
+// CSR SpMV (QEq real-space matrix times v) fused with the end of the matvec (as
 // qeq_finish_kernel): per row h = (recip + J_real v)_i + diag_i v_i + nn sum(v)
 // (+ slab terms), Hv_i = h, and the block sums of v.h and C.h into the CG
 // scalars -- one pass over the rows instead of two.

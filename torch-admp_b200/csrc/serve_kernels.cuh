@@ -5,7 +5,6 @@
 //   pair_ef   : warp per atom over its CSR row: Ewald real space (pme.py:312-349)
 //               and Gaussian damping (qeq.py:104-119) energy, force, potential
 //   csr_coef  : QEq real-space matrix entries ke (erfc(kappa r) - erfc(r / 2 eta_ij)) / r
-//   csr_spmv  : Hp += J_real p, eight lanes per row
 //   sys_terms : per-system self / non-neutral / damping-self / site energies
 #pragma once
 
@@ -585,78 +584,41 @@ static __global__ void __launch_bounds__(256)
     const T ei = eta[i];
     const long long st = pstart[i];
     const int n = pcnt[i];
-    for (int k = lane; k < n; k += 32) {
-      const int j = col[st + k];
-      T dr[3];
-      disp(fi, frac[j], bx, dr);
-      const T r = sqrt_t(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
-      const T ej = eta[j];
-      T eij = sqrt_t((ei * ei + ej * ej) * T(0.5));
-      if (eij == T(0)) eij = T(1e-10);
-      coef[st + k] = (T)ke * (erfc_t(kappa * r) - erfc_t(r / (T(2) * eij))) / r;
+    // three entries per lane per trip, their loads issued before any is used
+    for (int k0 = 0; k0 < n; k0 += 96) {
+      int jj[3];
+#pragma unroll
+      for (int u = 0; u < 3; ++u) {
+        const int k = k0 + lane + 32 * u;
+        jj[u] = k < n ? col[st + k] : -1;
+      }
+      T drr[3][3], ejj[3];
+#pragma unroll
+      for (int u = 0; u < 3; ++u) {
+        const int j = jj[u] >= 0 ? jj[u] : i;
+        disp(fi, frac[j], bx, drr[u]);
+        ejj[u] = eta[j];
+      }
+#pragma unroll
+      for (int u = 0; u < 3; ++u) {
+        if (jj[u] < 0) continue;
+        const T* dr = drr[u];
+        const T r = sqrt_t(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+        T eij = sqrt_t((ei * ei + ejj[u] * ejj[u]) * T(0.5));
+        if (eij == T(0)) eij = T(1e-10);
+        coef[st + k0 + lane + 32 * u] = (T)ke * (erfc_t(kappa * r) - erfc_t(r / (T(2) * eij))) / r;
+      }
     }
   }
 }
 
-// Hp[i] += sum_k coef[k] p[col[k]].  Eight lanes per row, four rows per warp
-// at a time; each lane issues the loads of up to kSpmvUnroll entries of its
-// row before using any of them, so a row costs about three dependent memory
-// latencies (row start, entries, gathered p) instead of three per 32
-// entries: the kernel is bound by the latency of those chains, not by bytes.
+// CSR SpMV layout (csr_spmv_finish_kernel): eight lanes per row, four rows
+// per warp at a time; each lane issues the loads of up to kSpmvUnroll entries
+// of its row before using any of them, so a row costs about three dependent
+// memory latencies (row start, entries, gathered p) instead of three per 32
+// entries: the SpMV is bound by the latency of those chains, not by bytes.
 constexpr int kSpmvLanes = 8;
 constexpr int kSpmvUnroll = 12;
-template <typename T>
-static __global__ void __launch_bounds__(256)
-    csr_spmv_kernel(Batch b, const long long* __restrict__ pstart, const int* __restrict__ pcnt,
-                    const int* __restrict__ col, const T* __restrict__ coef, const T* __restrict__ p,
-                    T* __restrict__ Hp, const int* __restrict__ done, int done_stride) {
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
-  if (done && done[(size_t)d.box_idx * done_stride]) return;
-  const int sub = threadIdx.x & (kSpmvLanes - 1);
-  const int grp = threadIdx.x / kSpmvLanes, ngrp = blockDim.x / kSpmvLanes;
-  const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
-  const int a1 = min(a0 + b.apb, d.natoms);
-  // every lane runs the same number of loop trips (shuffles below use the full mask);
-  // the next trip's row start and length are loaded while this trip's row is summed
-  long long st_next = 0;
-  int n_next = 0;
-  if (a0 + grp < a1) {
-    st_next = pstart[d.atom_off + a0 + grp];
-    n_next = pcnt[d.atom_off + a0 + grp];
-  }
-  for (int base = a0; base < a1; base += ngrp) {
-    const int a = base + grp;
-    const bool row = a < a1;
-    const int i = d.atom_off + (row ? a : a0);
-    const long long st = st_next;
-    const int n = row ? n_next : 0;
-    if (a + ngrp < a1) {
-      st_next = pstart[i + ngrp];
-      n_next = pcnt[i + ngrp];
-    }
-    T acc = 0;
-    for (int k0 = 0; k0 < n; k0 += kSpmvLanes * kSpmvUnroll) {
-      int c[kSpmvUnroll];
-      T w[kSpmvUnroll];
-#pragma unroll
-      for (int u = 0; u < kSpmvUnroll; ++u) {
-        const int k = k0 + sub + u * kSpmvLanes;
-        const bool ok = k < n;
-        c[u] = ok ? col[st + k] : -1;
-        w[u] = ok ? coef[st + k] : T(0);
-      }
-      T v[kSpmvUnroll];
-#pragma unroll
-      for (int u = 0; u < kSpmvUnroll; ++u) v[u] = c[u] >= 0 ? p[c[u]] : T(0);
-#pragma unroll
-      for (int u = 0; u < kSpmvUnroll; ++u) acc += w[u] * v[u];
-    }
-#pragma unroll
-    for (int o = kSpmvLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (row && sub == 0) Hp[i] += acc;
-  }
-}
 
 // block per system: self + non-neutral (+ damping self + site for QEq systems)
 template <typename T>

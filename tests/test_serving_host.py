@@ -1,5 +1,6 @@
 """Host-side scheduler pieces of the serving engine (no GPU): the interval
-allocator that places systems in the atom, pair and Green's-function pools."""
+allocator that places systems in the atom, pair and Green's-function pools,
+and the policy that decides which launched records the host waits for."""
 import numpy as np
 
 from admp_b200.serving import _Intervals
@@ -59,3 +60,57 @@ def test_intervals_first_fit_and_full_merge():
             iv.release(o, 10)
     iv.release(30, 25)
     assert iv.free == [(0, 100)]
+
+
+class _Ev:
+    """Stand-in for a CUDA event: `done` says whether the device passed it."""
+
+    def __init__(self, done):
+        self.done = done
+        self.waited = False
+
+    def query(self):
+        return self.done
+
+    def synchronize(self):
+        self.waited = True
+        self.done = True
+
+
+class _Sched:
+    """Just the state ServingEngine._drain reads and the completions it calls."""
+
+    def __init__(self, recs):
+        self._inflight = list(recs)
+        self.host_time = {"wait": 0.0, "results": 0.0}
+        self.completed = []
+
+    def _complete_finish(self, rec, now_fn):
+        self.completed.append(rec[2])
+
+    def _complete_iterate(self, rec):
+        self.completed.append(rec[2])
+
+
+def test_drain_keeps_the_current_steps_records_in_flight():
+    from admp_b200.serving import ServingEngine
+    drain = ServingEngine._drain
+    # no CG batch running: older records are waited for, the newest one (this step's) stays
+    s = _Sched([("finish", _Ev(False), "a"), ("finish", _Ev(False), "b"), ("finish", _Ev(False), "c")])
+    drain(s, None, 0, 1)
+    assert s.completed == ["a", "b"] and [r[2] for r in s._inflight] == ["c"]
+    # a record of this step whose event already passed completes without waiting
+    s = _Sched([("finish", _Ev(False), "a"), ("finish", _Ev(True), "b")])
+    drain(s, None, 0, 1)
+    assert s.completed == ["a", "b"] and not s._inflight
+    # a step that launched nothing waits for everything (no spinning on the host)
+    s = _Sched([("finish", _Ev(False), "a"), ("finish", _Ev(False), "b")])
+    drain(s, None, 0, 0)
+    assert s.completed == ["a", "b"] and not s._inflight
+    # CG batches running: the oldest records are waited for until one iterate record is
+    # outstanding; records after that complete only once their events passed
+    evs = [_Ev(False), _Ev(False), _Ev(False), _Ev(False)]
+    s = _Sched([("iter", evs[0], "i1"), ("finish", evs[1], "f1"), ("iter", evs[2], "i2"), ("finish", evs[3], "f2")])
+    drain(s, None, 1, 2)
+    assert s.completed == ["i1"] and [r[2] for r in s._inflight] == ["f1", "i2", "f2"]
+    assert evs[0].waited and not evs[1].waited and not evs[2].waited

@@ -62,8 +62,8 @@ class AdmpPools(ctypes.Structure):
 
 SERVE_CLUSTER_MATVEC = 1
 
-# ints per slot of the x-key tables (mesh planes along x + 1)
 _COPY_THREADS = 4  # host threads copying request arrays into the pinned staging buffers
+# ints per slot of the x-key tables (mesh planes along x + 1)
 XKEY_STRIDE = 1024
 
 
@@ -626,16 +626,21 @@ class ServingEngine:
             self._call(self.lib.admp_serve_qeq_finish, done)
             self._inflight.append(self._launch_finish(done))
 
-    def _drain(self, now_fn, max_iter_records: int) -> None:
+    def _drain(self, now_fn, max_iter_records: int, keep_new: int = 0) -> None:
         """Complete in-flight records in launch order: every record whose
         event has passed, and the oldest ones (waiting on them) while more than
-        `max_iter_records` iterate records are outstanding (all of them when
-        it is 0).  Keeping one iterate record in flight lets the host read
-        results while the device works on the next batch of CG iterations."""
+        `max_iter_records` iterate records are outstanding.  Keeping one
+        iterate record in flight lets the host read results while the device
+        works on the next batch of CG iterations.  With `max_iter_records` 0
+        (no CG batch running) all but the `keep_new` newest records are waited
+        for."""
         while self._inflight:
             rec = self._inflight[0]
-            n_iter = sum(1 for r in self._inflight if r[0] == "iter")
-            if max_iter_records > 0 and n_iter <= max_iter_records and not rec[1].query():
+            if max_iter_records > 0:
+                n_iter = sum(1 for r in self._inflight if r[0] == "iter")
+                if n_iter <= max_iter_records and not rec[1].query():
+                    break
+            elif len(self._inflight) <= keep_new and not rec[1].query():
                 break
             self._inflight.pop(0)
             h0 = time.perf_counter()
@@ -664,6 +669,7 @@ class ServingEngine:
         per-slot done flags); results of earlier steps are read afterwards,
         so the device stays busy while the host schedules."""
         n0 = len(self.results)
+        r0 = len(self._inflight)
         now = now_fn()
         h0 = time.perf_counter()
         new = self._admit(now)
@@ -688,7 +694,10 @@ class ServingEngine:
             ev.record(self.stream)
             self._inflight.append(("iter", ev, act, info))
         self.host_time["launch"] += time.perf_counter() - h1
-        self._drain(now_fn, 1 if self.active_qeq else 0)
+        # with arrived requests still waiting (a backlog), this step's records stay in flight so the
+        # next step's admission overlaps their device work; otherwise they are waited for at once
+        backlog = bool(self.queue) and self.queue[0][1] <= now
+        self._drain(now_fn, 1 if self.active_qeq else 0, len(self._inflight) - r0 if backlog else 0)
         self.stats["ticks"] += 1
         return len(self.results) - n0
 

@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--plain-sample", type=int, default=100)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--timeline", action="store_true",
+                    help="after the timed passes, trace one device-resident pass call by call (CUDA events "
+                         "around each library call) and print the accounting as JSON on stderr")
     return ap.parse_args()
 
 
@@ -373,6 +376,17 @@ def main():
     torch.cuda.synchronize()
     prof = L.profile_read()
     L.profile_enable(0)
+
+    if args.timeline:
+        ts0, ts1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        eng.call_trace = []
+        torch.cuda.synchronize()
+        ts0.record(st)
+        one_pass(dstream, to_host=False)
+        ts1.record(st)
+        torch.cuda.synchronize()
+        print(json.dumps({"timeline": eng.call_timeline(ts0, ts1)}), file=sys.stderr, flush=True)
+        eng.call_trace = None
 
     # e2e: host numpy inputs and results, closed loop
     h0 = eng.stats["h2d_bytes"]

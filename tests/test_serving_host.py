@@ -114,3 +114,27 @@ def test_drain_keeps_the_current_steps_records_in_flight():
     drain(s, None, 1, 2)
     assert s.completed == ["i1"] and [r[2] for r in s._inflight] == ["f1", "i2", "f2"]
     assert evs[0].waited and not evs[1].waited and not evs[2].waited
+
+
+class _TEv:
+    """Stand-in for a timing CUDA event recorded at device time t (ms)."""
+
+    def __init__(self, t):
+        self.t = t
+
+    def elapsed_time(self, other):
+        return other.t - self.t
+
+
+def test_call_timeline_accounts_spans_and_gaps():
+    from admp_b200.serving import ServingEngine
+
+    class _S:
+        call_trace = [("nb", _TEv(2.0), _TEv(5.0)), ("ef", _TEv(5.0), _TEv(9.0)), ("nb", _TEv(12.5), _TEv(14.0))]
+
+    tl = ServingEngine.call_timeline(_S(), _TEv(0.0), _TEv(15.0), top=2)
+    assert tl["pass_ms"] == 15.0
+    assert tl["calls"] == {"nb": {"n": 2, "ms": 4.5}, "ef": {"n": 1, "ms": 4.0}}
+    assert tl["gap_ms"] == 2.0 + 0.0 + 3.5 + 1.0
+    assert tl["largest_gaps"] == [{"ms": 3.5, "after": "ef", "before": "nb"},
+                                  {"ms": 2.0, "after": "start", "before": "nb"}]

@@ -260,6 +260,8 @@ class ServingEngine:
         self._stage_off = 0
         # host seconds per scheduler phase (admission + upload, launches, waiting on the device, reading results)
         self.host_time = {"admit": 0.0, "launch": 0.0, "wait": 0.0, "results": 0.0}
+        # when a list: (library call, start event, end event) of every call, for call_timeline()
+        self.call_trace = None
         # results as host numpy arrays (True) or device tensors (False)
         self.results_to_host = True
 
@@ -336,11 +338,41 @@ class ServingEngine:
         return out
 
     def _call(self, fn, items, *extra):
+        tr = self.call_trace
+        if tr is not None:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
         for ch in self._chunks(items):
             arr = self._sys_array(ch)
             st = fn(self.dt, ctypes.byref(self.pools), arr, len(ch), *extra, self.stream.cuda_stream)
             self.stats["launch_calls"] += 1
             L.check(st, fn.__name__)
+        if tr is not None:
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record(self.stream)
+            tr.append((fn.__name__, e0, e1))
+
+    def call_timeline(self, start, end, top: int = 3) -> dict:
+        """Device-side accounting of the calls traced between the events
+        `start` and `end` (recorded on the engine's stream around a pass, with
+        `call_trace` set to a list meanwhile): the stream time each library
+        call's work spans, and the gaps between calls, in which the device ran
+        only the engine's own copies or waited for the host."""
+        tr = self.call_trace or []
+        span, n = {}, {}
+        gaps = []
+        prev, prev_name = start, "start"
+        for name, e0, e1 in tr:
+            span[name] = span.get(name, 0.0) + e0.elapsed_time(e1)
+            n[name] = n.get(name, 0) + 1
+            gaps.append((prev.elapsed_time(e0), prev_name, name))
+            prev, prev_name = e1, name
+        gaps.append((prev.elapsed_time(end), prev_name, "end"))
+        gaps.sort(key=lambda g: -g[0])
+        return {"pass_ms": round(start.elapsed_time(end), 3),
+                "calls": {k: {"n": n[k], "ms": round(v, 3)} for k, v in span.items()},
+                "gap_ms": round(sum(g[0] for g in gaps), 3),
+                "largest_gaps": [{"ms": round(g[0], 3), "after": g[1], "before": g[2]} for g in gaps[:top]]}
 
     def _admit(self, now: float) -> List[_Active]:
         """Admit arrived requests while slots and pool space allow.  Within a

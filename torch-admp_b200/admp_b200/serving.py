@@ -699,7 +699,9 @@ class ServingEngine:
         energy + forces of newly admitted systems, then a batch of CG
         iterations over every active QEq system with a snapshot of the
         per-slot done flags); results of earlier steps are read afterwards,
-        so the device stays busy while the host schedules."""
+        so the device stays busy while the host schedules.  While arrived
+        requests wait, this step's launches are left in flight even with no
+        CG batch running, so the next step's admission overlaps them."""
         n0 = len(self.results)
         r0 = len(self._inflight)
         now = now_fn()

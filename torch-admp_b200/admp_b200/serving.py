@@ -252,6 +252,7 @@ class ServingEngine:
         self._retry: Dict[int, tuple] = {}
         self._inflight: List[tuple] = []  # launched work whose results are not read yet, in launch order
         self._zeros = {dt: torch.zeros(3 * 64, dtype=dt, device=self.dev) for dt in (torch.float32, torch.float64)}
+        self._zero_views = {}  # (dtype, rows, width) -> view of _zeros, the padding parts of _fill
         # upload scratch: box rows of one admission on the device, pinned host staging (ring of three)
         self._box_stage = {dt: torch.zeros(max_slots, 9, dtype=dt, device=self.dev)
                            for dt in (torch.float32, torch.float64)}
@@ -482,13 +483,25 @@ class ServingEngine:
         pads = pads or [0] * len(arrays)
         dtype = dest.dtype
         if isinstance(arrays[0], torch.Tensor):
+            # per part only the checks that decide whether a view is needed: a step admits hundreds of
+            # requests and a torch view costs more host time than the check
             parts = []
-            zero = self._zeros[dtype]
+            zv = self._zero_views
             for a, p in zip(arrays, pads):
-                a = a if a.dtype == dtype else a.to(dtype)
-                parts.append(a.reshape(-1, width) if width > 1 else a.reshape(-1))
+                if a.dtype != dtype:
+                    a = a.to(dtype)
+                if width > 1:
+                    if a.dim() != 2 or a.shape[1] != width:
+                        a = a.reshape(-1, width)
+                elif a.dim() != 1:
+                    a = a.reshape(-1)
+                parts.append(a)
                 if p:
-                    parts.append(zero[:p * width].view(p, width) if width > 1 else zero[:p])
+                    z = zv.get((dtype, p, width))
+                    if z is None:
+                        z = self._zeros[dtype][:p * width]
+                        z = zv[(dtype, p, width)] = z.view(p, width) if width > 1 else z
+                    parts.append(z)
             torch.cat(parts, out=dest.view(-1, width) if width > 1 else dest.view(-1))
             return 0
         npdt = {torch.float32: np.float32, torch.float64: np.float64}[dtype]

@@ -1,6 +1,7 @@
 """Host-side scheduler pieces of the serving engine (no GPU): the interval
 allocator that places systems in the atom, pair and Green's-function pools,
-and the policy that decides which launched records the host waits for."""
+the policy that decides which launched records the host waits for, the call
+timeline accounting and the packing of request arrays into pool slices."""
 import numpy as np
 
 from admp_b200.serving import _Intervals
@@ -138,3 +139,30 @@ def test_call_timeline_accounts_spans_and_gaps():
     assert tl["gap_ms"] == 2.0 + 0.0 + 3.5 + 1.0
     assert tl["largest_gaps"] == [{"ms": 3.5, "after": "ef", "before": "nb"},
                                   {"ms": 2.0, "after": "start", "before": "nb"}]
+
+
+def test_fill_device_tensor_parts_with_padding():
+    """_fill's tensor branch (what admission uses for device-resident requests), run on CPU tensors:
+    every request array lands at its offset, reshaped to the pool's row width and converted to the
+    pool's dtype, with zero rows in the alignment gaps."""
+    import torch
+    from admp_b200.serving import ServingEngine
+
+    class _S:
+        _zeros = {dt: torch.zeros(3 * 64, dtype=dt) for dt in (torch.float32, torch.float64)}
+        _zero_views = {}
+
+    rng = np.random.default_rng(5)
+    for width, shapes in ((3, [(4, 3), (7, 3), (1, 3)]), (1, [(5,), (2,), (3,)]), (9, [(3, 3), (3, 3)])):
+        for dt in (torch.float32, torch.float64):
+            arrays = [torch.tensor(rng.standard_normal(sh), dtype=torch.float64) for sh in shapes]
+            pads = [int(rng.integers(0, 4)) for _ in shapes[:-1]] + [0]
+            rows = sum(a.numel() // width + p for a, p in zip(arrays, pads))
+            dest = torch.full((rows * width,), float("nan"), dtype=dt)
+            for _ in range(2):  # the second call reuses the cached padding views
+                assert ServingEngine._fill(_S(), dest, arrays, pads, width) == 0
+                ref = []
+                for a, p in zip(arrays, pads):
+                    ref.append(a.reshape(-1).to(dt))
+                    ref.append(torch.zeros(p * width, dtype=dt))
+                assert torch.equal(dest, torch.cat(ref))

@@ -195,3 +195,35 @@ def test_serving_triclinic_cells_match_oracle(cuda, dtype, etol, ftol, qtol):
         assert np.abs(out.forces - F).max() / np.abs(F).max() < ftol, r.rid
         if q is not None:
             assert np.abs(out.charges - q).max() < qtol, r.rid
+
+
+def test_serving_small_steps_with_backlog_and_call_timeline(cuda, stream_and_oracle):
+    """Two admissions per step: PME-only steps run while requests still wait, so their launches stay
+    in flight across steps.  Every result still matches the oracle, and the call timeline splits the
+    pass into the calls' spans and the gaps between them."""
+    from admp_b200.serving import ServingEngine
+    reqs, refs = stream_and_oracle
+    eng = ServingEngine(dtype=torch.float32, max_atoms=200_000, max_slots=64, mesh_budget=4_000_000, tol=1e-7,
+                        admit_per_tick=2)
+    eng.call_trace = []
+    st = eng.stream
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(st)
+    out = {r.rid: r for r in eng.run(reqs, arrivals=False)}
+    s1.record(st)
+    torch.cuda.synchronize()
+    assert len(out) == len(reqs) and eng.stats["ticks"] >= len(reqs) // 2
+    for r, (E, F, q) in zip(reqs, refs):
+        o = out[r.rid]
+        assert o.status == 0
+        assert abs(o.energy - E) / abs(E) < 1e-5, (r.kind, o.energy, E)
+        assert np.abs(o.forces - F).max() / np.abs(F).max() < 1e-4
+        if q is not None:
+            assert np.abs(o.charges - q).max() < 1e-5
+    tl = eng.call_timeline(s0, s1)
+    assert tl["calls"]["admp_serve_neighbors"]["n"] >= len(reqs) // 2
+    total = sum(c["ms"] for c in tl["calls"].values()) + tl["gap_ms"]
+    assert abs(total - tl["pass_ms"]) < 0.1 + 1e-3 * tl["pass_ms"]
+    assert all(g["ms"] >= 0.0 for g in tl["largest_gaps"])
+    eng.call_trace = None
+    assert eng.atoms.used() == 0 and not eng._inflight

@@ -227,6 +227,26 @@ int admp_qeq_solve(int dtype, int flags, int natoms, const int* kmesh, const voi
                    int* iters, double* resid, void* workspace, size_t workspace_bytes,
                    void* stream);
 
+/* Several frames of the same atom count in one solve (the differentiation */
+/* batch: jittered frames of one system, and the implicit adjoint of their   */
+/* charges).  The reference solves one frame per pgrad_optimize call          */
+/* (qeq.py:1117-1270); per frame the arithmetic and the stopping rule are the */
+/* same as admp_qeq_solve.  Frame f holds atoms [f N, (f+1) N) of pos, chi,   */
+/* hardness, eta, rhs_shift and q, box f, and mesh kmesh[3f .. 3f+2] (HOST    */
+/* [nframes, 3]); pairs index atoms over all frames (frame f's pairs use     */
+/* indices f N + i); C [n_const, N] and b (HOST [n_const]) are shared by      */
+/* every frame.  iters, resid: HOST [nframes] or NULL.  nframes <= 256.       */
+size_t admp_qeq_frames_workspace_size(int dtype, int nframes, int natoms, long long npairs,
+                                      const int* kmesh, int n_const);
+int admp_qeq_solve_frames(int dtype, int flags, int nframes, int natoms, const int* kmesh,
+                          const void* pos, const void* box, long long npairs,
+                          const long long* pairs, const void* ds, const void* buffer_scales,
+                          const void* chi, const void* hardness, const void* eta,
+                          const void* rhs_shift, double kappa, double ke, int n_const,
+                          const void* C, const double* b, void* q, double tol, int max_iter,
+                          int* iters, double* resid, void* workspace, size_t workspace_bytes,
+                          void* stream);
+
 /* Hessian-vector product of the same quadratic form (dE/dq at p minus at   */
 /* 0): out [N] = H p.  Used by the implicit adjoint of the charge solve.      */
 int admp_qeq_hvp(int dtype, int flags, int natoms, const int* kmesh, const void* pos,
@@ -304,21 +324,8 @@ typedef struct admp_pools {
   double* pos64;       /* [A,3] or NULL */
   double* box64;       /* [S,3,3] or NULL */
   void* frac64;        /* [A] double4 scratch, needed with pos64 */
-  /* optional per-slot x-key tables of QEq slots (used with
-   * ADMP_SERVE_CLUSTER_MATVEC): the atoms of a QEq system sorted by their
-   * first mesh plane along x (in `sorted`) and the start of each plane key,
-   * which let one thread-block cluster per system run the whole
-   * reciprocal-space matvec of a CG iteration in shared memory.  Slots whose
-   * K0 + 1 exceeds xkey_stride use the mesh passes. */
-  int* xkey;           /* [S, xkey_stride] */
-  int xkey_stride;
-  int flags;           /* ADMP_SERVE_* below */
+  int flags;           /* reserved, 0 */
 } admp_pools;
-
-/* admp_pools.flags: run each CG matvec of QEq slots as one cluster-resident
- * kernel per system (needs xkey); otherwise the matvec is the atom-parallel
- * spread, the FFT passes and the atom-parallel gather. */
-#define ADMP_SERVE_CLUSTER_MATVEC 1
 
 size_t admp_serve_slot_state_bytes(void);
 size_t admp_serve_sys_scratch_bytes(int nsys);

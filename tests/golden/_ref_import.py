@@ -5,12 +5,21 @@ The reference needs ``ase.units``, ``torchopt`` and a generated
 exactly what the reference uses of them (eV/Angstrom units, a forward-only
 ``custom_root`` decorator).  Used by ``make_golden.py`` in this directory,
 never at test time and never on the GPU host.
+
+The checkout is named by the environment variable ``TORCH_ADMP_REFERENCE``
+(the directory that holds ``src/torch_admp`` and ``tests/data``).
 """
 import os
 import sys
 import types
 
-REF_SRC = "/root/reference/src"
+
+def reference_root() -> str:
+    root = os.environ.get("TORCH_ADMP_REFERENCE")
+    if not root or not os.path.isdir(os.path.join(root, "src", "torch_admp")):
+        raise SystemExit("set TORCH_ADMP_REFERENCE to a torch-admp checkout (the directory holding "
+                         "src/torch_admp and tests/data), e.g. TORCH_ADMP_REFERENCE=../torch-admp")
+    return root
 
 
 def import_reference():
@@ -39,7 +48,8 @@ def import_reference():
         "ase": ase, "ase.units": units, "torchopt": to, "torchopt.diff": diff,
         "torchopt.diff.implicit": imp, "torchopt.linear_solve": ls, "torch_admp._version": ver,
     })
-    if REF_SRC not in sys.path:
-        sys.path.insert(0, REF_SRC)
+    ref_src = os.path.join(reference_root(), "src")
+    if ref_src not in sys.path:
+        sys.path.insert(0, ref_src)
     import torch_admp  # noqa: F401
     return torch_admp

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory by running the reference.
 
-Run in the development container only (it reads the read-only reference
-checkout):  ``python tests/golden/make_golden.py [case ...]``.
+Run where a torch-admp checkout is available (it imports the reference):
+``TORCH_ADMP_REFERENCE=<checkout> python tests/golden/make_golden.py [case ...]``.
 
 Each ``*.npz`` holds the inputs of one case together with what the
 reference's own FP64 CPU path (torch-admp 1.1.5, imported through
@@ -22,10 +22,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
 sys.path.insert(0, os.path.join(REPO, "torch-admp_b200"))
-REF_DATA = "/root/reference/tests/data"
 SEED = 1024
 
-from _ref_import import import_reference  # noqa: E402
+from _ref_import import import_reference, reference_root  # noqa: E402
+
+REF_DATA = os.path.join(reference_root(), "tests", "data")
 
 import_reference()
 import torch  # noqa: E402
@@ -353,6 +354,112 @@ def case_electrode(name):
          lammps_eta=1.6, rcut=rcut, kappa=0.5, ethresh=1e-6)
 
 
+def electrode_cfg3_inputs(n_side=24, n_ions=3000, seed=SEED):
+    """Two fcc(111) slabs of 2 x n_side^2 atoms, n_ions +-1 ions in a 40 A gap,
+    Lz = 3 x slab extent, electrode Gaussian width 0.5 A (LAMMPS eta sqrt 2),
+    CONP at 1 V (top) and 0 V (bottom), total electrode charge 0 (symm)."""
+    pos, box, q, top, bot = synthetic.electrode_system(seed, n_side=n_side, n_ions=n_ions)
+    cons = [(int(top[0]), int(top[-1]) + 1, 1.0, "conp"), (int(bot[0]), int(bot[-1]) + 1, 0.0, "conp")]
+    return pos, box, q, cons
+
+
+def case_electrode_cfg3():
+    """Constant-potential electrodes at their stated size: 2 x 1,152 electrode
+    atoms, 3,000 ions, 64 x 64 x 160 mesh, slab correction along z."""
+    pos, box, q, cons = electrode_cfg3_inputs()
+    rcut, ethresh, kmesh = 6.0, 5e-4, [64, 64, 160]
+    calc = PolarizableElectrode(rcut=rcut, ethresh=ethresh, kmesh=kmesh, slab_corr=True, eps=1e-8, ls_eps=1e-8,
+                                max_iter=400)
+    p = T(pos, True)
+    b = T(box)
+    ch = T(q, True)
+    nb = TorchNeighborList(rcut)
+    pairs = nb(p, b)
+    lc = [LAMMPSElectrodeConstraint(indices=np.arange(a, z), value=v, mode=md, eta=np.sqrt(2.0)) for (a, z, v, md)
+          in cons]
+    data = setup_from_lammps(len(q), lc, True)
+    t0 = time.time()
+    E, F, qo = infer(calc, p, b, ch, pairs, nb.get_ds(), nb.get_buffer_scales(), *data, method="lbfgs")
+    print("electrode_cfg3 lbfgs", time.time() - t0, "s, E", float(E), flush=True)
+    save("electrode_cfg3", pos=pos, box=box, q_in=q, E=np.asarray(E.detach()), forces=F.detach().numpy(),
+         q_ref=qo.detach().numpy(), cons=np.array([[a, z, v, 0] for (a, z, v, md) in cons]), lammps_eta=np.sqrt(2.0),
+         rcut=rcut, ethresh=ethresh, kmesh=np.array(kmesh), eps=1e-8, time_ref_s=time.time() - t0,
+         threads=torch.get_num_threads())
+
+
+def case_qeq_cfg4():
+    """Energy gradients of the differentiation batch at the solved charges:
+    frames 0 and 1 of the jittered 1,000-water system (3,000 atoms, 31 A box,
+    48^3 mesh, rc 6).  The reference evaluates E at the detached optimum
+    (qeq.py:1262-1268), so its autograd gradient is the total derivative
+    (the charge response drops out at the constrained minimum).  eps 1e-8:
+    at 1e-9 the reference's nonlinear CG ran 374 iterations on frame 0 and
+    left the total-charge constraint (E -2760 instead of -209.9 eV)."""
+    pos_f, box_f, chi, hard, eta, _ = synthetic.water_frames(2, SEED)
+    out = {}
+    for f in range(2):
+        p = T(pos_f[f], True)
+        b = T(box_f[f], True)
+        c, h, e = T(chi, True), T(hard, True), T(eta, True)
+        nb = TorchNeighborList(6.0)
+        pairs = nb(p, b)
+        ds = nb.get_ds()
+        bs = nb.get_buffer_scales()
+        n = pos_f.shape[1]
+        mod = QEqForceModule(6.0, 5e-4, kmesh=48, eps=1e-8, ls_eps=1e-8, max_iter=400)
+        t0 = time.time()
+        E, q = pgrad_optimize(mod, torch.zeros(n), p, b, c, h, e, pairs, ds, bs, torch.ones((1, n)), torch.zeros(1),
+                              reinit_q=True, method="quadratic")
+        g = torch.autograd.grad(E.sum(), [p, b, c, h, e])
+        assert 0 <= mod.converge_iter < 400 and abs(float(q.sum())) < 1e-9
+        print("qeq_cfg4 frame", f, "iters", mod.converge_iter, "t", time.time() - t0, "E", float(E.sum()), flush=True)
+        for k, v in zip(("dpos", "dbox", "dchi", "dhard", "deta"), g):
+            out[f"{k}_{f}"] = v.numpy()
+        out[f"E_{f}"] = E.detach().numpy()
+        out[f"q_{f}"] = q.detach().numpy()
+        out[f"iters_{f}"] = mod.converge_iter
+    save("qeq_cfg4", pos=pos_f, box=box_f, chi=chi, hardness=hard, eta=eta, rcut=6.0, ethresh=5e-4, kmesh=48, **out)
+
+
+def case_qeq_dq_dchi():
+    """dq/dchi through the reference's dense KKT solve, which stays
+    differentiable in chi (QEqForceModule.solve_matrix_inversion,
+    qeq.py:517-607): 64 waters (192 atoms) in a 12.4 A box, loss
+    L = sum_i w_i q_i with seeded weights w."""
+    pos, box, chi, hard, eta, _ = synthetic.water_system(64, 12.4, SEED + 6)
+    n = pos.shape[0]
+    w = np.random.default_rng(SEED + 8).normal(size=n)
+    p, b = T(pos), T(box)
+    c = T(chi, True)
+    nb = TorchNeighborList(6.0)
+    pairs = nb(p, b)
+    mod = QEqForceModule(6.0, 5e-4, kmesh=20)
+    E, q, _, _ = mod.solve_matrix_inversion(p, b, c, T(hard), T(eta), pairs, nb.get_ds(), nb.get_buffer_scales(),
+                                           torch.ones((1, n)), torch.zeros(1))
+    loss = (q * T(w)).sum()
+    (gchi,) = torch.autograd.grad(loss, [c])
+    save("qeq_dq_dchi", pos=pos, box=box, chi=chi, hardness=hard, eta=eta, w=w, q=q.detach().numpy(),
+         dL_dchi=gchi.numpy(), rcut=6.0, ethresh=5e-4, kmesh=20)
+
+
+def case_ewald_params():
+    """setup_ewald_parameters (pme.py:564-658) over both methods, several
+    cut-offs, thresholds, spacings and orthogonal boxes."""
+    from torch_admp.pme import setup_ewald_parameters
+    rows = []
+    for rcut in (4.0, 5.0, 6.0, 9.5):
+        for thr in (1e-3, 5e-4, 1e-5, 1e-7):
+            for L in ((10.0, 10.0, 10.0), (25.0, 31.0, 58.5), (69.24, 59.96, 140.1)):
+                box = np.diag(L)
+                k, kx, ky, kz = setup_ewald_parameters(rcut, box, thr, method="openmm")
+                rows.append([0, rcut, thr, 0.0, *L, k, kx, ky, kz])
+                for sp in (0.5, 1.0, 1.37):
+                    k, kx, ky, kz = setup_ewald_parameters(rcut, box, thr, spacing=sp, method="gromacs")
+                    rows.append([1, rcut, thr, sp, *L, k, kx, ky, kz])
+    save("ewald_params", rows=np.array(rows, dtype=np.float64),
+         columns=np.array(["method", "rcut", "threshold", "spacing", "Lx", "Ly", "Lz", "kappa", "kx", "ky", "kz"]))
+
+
 def case_nblist():
     rng = np.random.default_rng(SEED + 7)
     out = {}
@@ -381,6 +488,8 @@ CASES = {
     "pme_kspace": case_pme_kspace, "pme_slab": case_pme_slab, "obc": case_obc,
     "slab_lammps": case_slab_lammps, "damping_site": case_damping_site, "qeq_small": case_qeq_small,
     "qeq_water_small": case_qeq_water_small, "qeq_water_cfg2": case_qeq_water_cfg2, "nblist": case_nblist,
+    "electrode_cfg3": case_electrode_cfg3, "ewald_params": case_ewald_params,
+    "qeq_cfg4": case_qeq_cfg4, "qeq_dq_dchi": case_qeq_dq_dchi,
 }
 for _n in ELECTRODE_CASES:
     CASES["electrode_" + _n] = (lambda nm: (lambda: case_electrode(nm)))(_n)

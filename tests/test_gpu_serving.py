@@ -112,36 +112,6 @@ def _qeq_sizes(nmin, nmax, k, seed=5):
     return [reqs[int(i * (len(reqs) - 1) / (k - 1))] for i in range(k)]
 
 
-@pytest.mark.parametrize("dtype,nmax,qtol,etol", [(torch.float32, 6000, 2e-6, 1e-6),
-                                                  (torch.float32, 20000, 2e-6, 1e-6),
-                                                  (torch.float64, 3000, 1e-9, 1e-11)])
-def test_cluster_matvec_matches_mesh_passes(cuda, dtype, nmax, qtol, etol):
-    """The cluster-resident reciprocal matvec (whole mesh in the shared memory
-    of one thread-block cluster per system) gives the charges of the mesh
-    passes (spread, FFT passes, gather through global memory)."""
-    from admp_b200 import _lib as L
-    from admp_b200.serving import ServingEngine
-    reqs = _qeq_sizes(300, nmax, 5)
-    out = {}
-    for fused in (True, False):
-        eng = ServingEngine(dtype=dtype, max_atoms=200_000, max_slots=16, mesh_budget=4_000_000,
-                            tol=1e-10 if dtype == torch.float64 else 1e-7, fused_recip=fused)
-        L.profile_enable(100000)
-        res = eng.run(reqs, arrivals=False)
-        torch.cuda.synchronize()
-        prof = L.profile_read()
-        L.profile_enable(0)
-        out[fused] = ({r.rid: r for r in res}, prof["recip_fused"]["launches"])
-    assert out[False][1] == 0
-    if nmax <= 6000:  # clusters of at most 4 CTAs hold these meshes
-        assert out[True][1] > 0
-    for r in reqs:
-        a, b = out[True][0][r.rid], out[False][0][r.rid]
-        assert a.status == 0 and b.status == 0
-        assert np.abs(a.charges - b.charges).max() < qtol, (r.natoms, np.abs(a.charges - b.charges).max())
-        assert abs(a.energy - b.energy) / abs(b.energy) < etol, (r.natoms, a.energy, b.energy)
-
-
 def test_row_overflow_is_served_again(cuda, stream_and_oracle):
     """Neighbour rows live in fixed per-atom slots sized from the mean density;
     a request whose rows outgrow them comes back with ADMP_ERR_CAPACITY and the

@@ -124,3 +124,39 @@ def test_oracle_qeq(name, kmesh):
     qq, conv = O.solve_quadratic(s, np.zeros(n), C, b, max_iter=100, eps=1e-6)
     assert conv == int(d["iters_quadratic"])
     assert np.abs(qq - d["q_quadratic"]).max() < 1e-9
+
+
+def electrode_cfg3_case():
+    """Inputs of the golden constant-potential run at its stated size (two
+    fcc(111) slabs of 1,152 atoms, 3,000 ions, 64 x 64 x 160 mesh, slab
+    correction), regenerated from the seeded generator and checked against the
+    stored copy."""
+    from admp_b200 import synthetic
+    d = golden("electrode_cfg3")
+    pos, box, q, top, bot = synthetic.electrode_system(1024)
+    assert np.array_equal(pos, d["pos"]) and np.array_equal(box, d["box"]) and np.array_equal(q, d["q_in"])
+    cons = [dict(indices=np.arange(int(a), int(z)), mode="conp", value=float(v), eta=float(d["lammps_eta"]))
+            for a, z, v, _ in d["cons"]]
+    assert [c["indices"][0] for c in cons] == [top[0], bot[0]]
+    return d, pos, box, q, cons
+
+
+def test_oracle_electrode_cfg3_matches_reference():
+    """The oracle's constant-potential solve (projected linear CG to
+    ||P grad||/N < 1e-10) against the reference's infer(method="lbfgs", eps
+    1e-8) on the full 5,304-atom system: the charges agree to the reference's
+    own convergence (~5e-7 e), energy and forces far tighter."""
+    d, pos, box, q, cons = electrode_cfg3_case()
+    rc = float(d["rcut"])
+    pairs = O.nblist_pbc(pos, box, rc)
+    ds = O.pairs_ds(pos, pairs, box)
+    bs = O.pair_buffer_scales(pairs)
+    mask, eta, chi, hard, C, b, ffm, ffp = O.setup_from_lammps(len(q), cons, True)
+    assert mask.sum() == 2304 and np.allclose(eta[mask], 0.5)
+    E, F, qo = O.electrode_infer(pos, box, q, pairs, ds, bs, mask, eta, chi, hard, C, b, ffm, ffp, rcut=rc,
+                                 ethresh=float(d["ethresh"]), kmesh=d["kmesh"].tolist(), slab_corr_flag=True,
+                                 solver="cg", tol=1e-10)
+    assert abs(E - float(d["E"])) / abs(float(d["E"])) < 1e-8
+    assert rel(F, d["forces"]) < 1e-6
+    assert np.abs(qo - d["q_ref"]).max() < 1e-6
+    assert abs(qo[mask].sum()) < 1e-10

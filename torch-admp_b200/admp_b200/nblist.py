@@ -137,3 +137,25 @@ def sort_pairs(pairs: torch.Tensor) -> torch.Tensor:
     pairs = pairs[idx]
     idx = torch.argsort(pairs[:, 0], stable=True)
     return pairs[idx]
+
+
+def frame_pair_lists(positions: torch.Tensor, box: torch.Tensor, cutoff: float):
+    """Neighbour lists of nf frames stacked for the multi-frame calls:
+    pairs [nf, P, 2] (frame-local indices), ds [nf, P] (differentiable with
+    respect to positions [nf, N, 3] and box [nf, 3, 3]) and buffer_scales
+    [nf, P], with P the longest frame's list; the rows past a frame's own
+    pairs hold (0, 0) with distance 1 and scale 0, which every kernel skips."""
+    nf = positions.shape[0]
+    lists = []
+    for f in range(nf):
+        nb = TorchNeighborList(cutoff)
+        pr = nb(positions[f], box[f])
+        lists.append((pr, nb.get_ds(), nb.get_buffer_scales()))
+    P = max(int(p.shape[0]) for p, _, _ in lists)
+    pairs, ds, bs = [], [], []
+    for pr, d, s in lists:
+        pad = P - int(pr.shape[0])
+        pairs.append(torch.cat([pr, pr.new_zeros(pad, 2)]))
+        ds.append(torch.cat([d, d.new_ones(pad)]))
+        bs.append(torch.cat([s, s.new_zeros(pad)]))
+    return torch.stack(pairs), torch.stack(ds), torch.stack(bs)

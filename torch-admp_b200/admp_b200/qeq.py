@@ -414,3 +414,176 @@ def qeq_solve(module: QEqForceModule, positions, box, chi, hardness, eta, pairs,
     return QEqSolveFn.apply(positions, box, chi, hardness, eta, ds, shift, module, pairs, buffer_scales,
                             constraint_matrix, constraint_vals, q0, module.eps if tol is None else tol,
                             module.max_iter if max_iter is None else max_iter)
+
+
+# ---------------------------------------------------------------------------
+# several frames in one solve (the differentiation batch)
+# ---------------------------------------------------------------------------
+def _frames_vec(v, nf: int, n: int, dt):
+    """[N] (shared by the frames) or [nf, N] -> contiguous [nf * N] of dtype dt."""
+    return prep_float(v.detach().reshape(-1, n).expand(nf, n), dt).reshape(-1)
+
+
+def _qeq_solve_frames_raw(module, q0, positions, box, chi, hardness, eta, pairs, ds, buffer_scales, C, b, project_q0,
+                          tol, max_iter, shift=None):
+    """admp_qeq_solve_frames over positions [nf, N, 3], box [nf, 3, 3], pairs
+    [nf, P, 2] (frame-local indices, padding rows with scale 0), ds / scales
+    [nf, P]; chi, hardness, eta, shift [N] or [nf, N].  Returns (q [nf, N],
+    iterations [nf], residuals [nf], status)."""
+    lib = L.load()
+    L.require_cuda(positions, "positions")
+    if box is None:
+        raise ValueError("admp_b200 QEq solve needs a periodic box")
+    nf, n = int(positions.shape[0]), int(positions.shape[1])
+    dt = positions.dtype
+    dev = positions.device
+    ec = module.const_lib.energy_coeff
+    lc = module.const_lib.length_coeff
+    pos = prep_float(positions.detach() * lc, dt)
+    bx = prep_float(box.detach().reshape(nf, 3, 3) * lc, dt)
+    P = int(pairs.shape[1])
+    offs = (torch.arange(nf, device=dev, dtype=torch.long) * n).view(nf, 1, 1)
+    prg = (pairs.to(torch.long) + offs).reshape(-1, 2).contiguous()
+    dsc = prep_float(ds.detach() * lc, dt).reshape(-1)
+    bsc = prep_float(buffer_scales.reshape(nf, P), dt).reshape(-1)
+    chi_c = _frames_vec(chi * ec, nf, n, dt)
+    hard_c = _frames_vec(hardness * ec, nf, n, dt)
+    eta_c = _frames_vec(eta * lc, nf, n, dt) if eta is not None else torch.zeros(nf * n, dtype=dt, device=dev)
+    sh = _frames_vec(shift, nf, n, dt) if shift is not None else None
+    q = _frames_vec(q0, nf, n, dt).clone()
+    flags = module._flags()
+    if project_q0:
+        flags |= L.QEQ_PROJECT_Q0
+    c = module.submodels["coulomb"]
+    km = [[1, 1, 1]] * nf
+    if c.kspace_flag:
+        km = c.kmesh_for(bx)
+        c._kmesh = torch.tensor(km[-1], dtype=torch.long)
+    kp, _keep = L.int3([k for row in km for k in row])
+    nc = 0 if C is None else int(C.shape[0])
+    Cc = prep_float(C.detach().reshape(nc, n), dt) if nc else None
+    bvals = (ctypes.c_double * max(nc, 1))(*([float(v) for v in b.detach().reshape(-1).tolist()] if nc else [0.0]))
+    nbytes = lib.admp_qeq_frames_workspace_size(L.dtype_code(dt), nf, n, nf * P, kp if c.kspace_flag else None, nc)
+    if nbytes == 0:
+        L.check(L.BAD_ARG, f"QEq workspace for {nf} frames")
+    ws = L.workspace(nbytes, dev)
+    iters = (ctypes.c_int * nf)()
+    resid = (ctypes.c_double * nf)()
+    st = lib.admp_qeq_solve_frames(L.dtype_code(dt), flags, nf, n, kp, L.ptr(pos), L.ptr(bx), nf * P, L.ptr(prg),
+                                   L.ptr(dsc), L.ptr(bsc), L.ptr(chi_c), L.ptr(hard_c), L.ptr(eta_c), L.ptr(sh),
+                                   float(c.kappa) or 1.0, module.const_lib.dielectric, nc, L.ptr(Cc), bvals, L.ptr(q),
+                                   float(tol), int(max_iter), iters, resid, L.ptr(ws), nbytes, L.stream_of(dev))
+    if st == L.NOT_CONVERGED:
+        L.warn_not_converged(lib.admp_last_error_message().decode())
+    elif st != L.OK:
+        L.check(st, "QEq solve (frames)")
+    return q.reshape(nf, n), list(iters), list(resid), st
+
+
+def _quadratic_part_grads_frames(module, pos, bx, pr, dsc, bsc, q, eta_c):
+    """Gradients of E_J(q) = Coulomb + damping over nf frames w.r.t. positions
+    [nf, N, 3], box [nf, 3, 3], ds [nf, P] and eta [nf, N]."""
+    c = module.submodels["coulomb"]
+    km = c.kmesh_for(bx) if c.kspace_flag else [[1, 1, 1]] * pos.shape[0]
+    qf = q.contiguous()
+    _, _, g = coulomb_pbc(pos, bx, pr, dsc, bsc, qf, float(c.kappa), km, module.const_lib.dielectric, c.rspace_flag,
+                          c.kspace_flag, c.slab_corr_flag, c.slab_axis, True)
+    out = {"pos": g["pos"], "box": g["box"], "ds": g["ds"], "eta": torch.zeros_like(qf)}
+    if "damping" in module.submodels:
+        _, gds, _, geta = damping_raw(dsc, qf, eta_c, pr, bsc, module.const_lib.dielectric, True)
+        out["ds"] = out["ds"] + gds
+        out["eta"] = geta
+    return out
+
+
+class QEqFramesFn(torch.autograd.Function):
+    """Charges q*[nf, N] of several frames, differentiable through the implicit
+    adjoint (one batched second CG over all frames)."""
+
+    @staticmethod
+    def forward(ctx, positions, box, chi, hardness, eta, ds, shift, module, pairs, buffer_scales, C, b, q0, tol,
+                max_iter):
+        q, iters, resid, status = _qeq_solve_frames_raw(module, q0, positions, box, chi, hardness, eta, pairs, ds,
+                                                        buffer_scales, C, b, True, tol, max_iter, shift)
+        module.converge_iter = max(iters) if status == L.OK else -1
+        module.frame_iters = iters
+        module.frame_residuals = resid
+        module.last_residual = max(resid)
+        ctx.module = module
+        ctx.tol = tol
+        ctx.max_iter = max_iter
+        ctx.save_for_backward(positions, box, chi, hardness, eta, ds, pairs, buffer_scales,
+                              C if C is not None else torch.empty(0), q)
+        ctx.has_C = C is not None
+        return q
+
+    @staticmethod
+    def backward(ctx, gq):
+        positions, box, chi, hardness, eta, ds, pairs, bs, C, q = ctx.saved_tensors
+        module = ctx.module
+        Cm = C if ctx.has_C else None
+        zero_b = torch.zeros(Cm.shape[0], dtype=q.dtype, device=q.device) if Cm is not None else None
+        lam, _, _, _ = _qeq_solve_frames_raw(module, torch.zeros_like(q), positions, box, -gq.detach(), hardness, eta,
+                                             pairs, ds, bs, Cm, zero_b, True, min(ctx.tol, 1e-8),
+                                             max(ctx.max_iter, 200))
+        lam = lam.to(q.dtype)
+        out = [None] * 15
+        ec = module.const_lib.energy_coeff
+        if ctx.needs_input_grad[2]:
+            out[2] = -lam
+        if ctx.needs_input_grad[6]:
+            out[6] = -lam / ec
+        if ctx.needs_input_grad[3]:
+            out[3] = -2.0 * q * lam
+        if any(ctx.needs_input_grad[i] for i in (0, 1, 4, 5)):
+            nf, n = q.shape
+            dt = positions.dtype
+            lc0 = module.const_lib.length_coeff
+            pos = prep_float(positions.detach() * lc0, dt)
+            bx = prep_float(box.detach() * lc0, dt)
+            pr = pairs.to(torch.long).contiguous()
+            dsc = prep_float(ds.detach() * lc0, dt)
+            bsc = prep_float(bs, dt)
+            eta_c = _frames_vec(eta * lc0, nf, n, dt).reshape(nf, n)
+            gp = _quadratic_part_grads_frames(module, pos, bx, pr, dsc, bsc, q + lam, eta_c)
+            gm = _quadratic_part_grads_frames(module, pos, bx, pr, dsc, bsc, q - lam, eta_c)
+            lc = lc0 / ec
+            if ctx.needs_input_grad[0]:
+                out[0] = -0.5 * (gp["pos"] - gm["pos"]) * lc
+            if ctx.needs_input_grad[1]:
+                out[1] = -0.5 * (gp["box"] - gm["box"]) * lc
+            if ctx.needs_input_grad[5]:
+                out[5] = -0.5 * (gp["ds"] - gm["ds"]) * lc
+            if ctx.needs_input_grad[4]:
+                out[4] = -0.5 * (gp["eta"] - gm["eta"]) * lc
+        return tuple(out)
+
+
+def qeq_solve_frames(module: QEqForceModule, positions, box, chi, hardness, eta, pairs, ds, buffer_scales,
+                     constraint_matrix=None, constraint_vals=None, q0=None, shift=None, tol: Optional[float] = None,
+                     max_iter: Optional[int] = None):
+    """Differentiable QEq charges of nf frames of N atoms in one batched solve.
+
+    positions [nf, N, 3], box [nf, 3, 3], pairs [nf, P, 2] with frame-local
+    atom indices (rows beyond a frame's own pairs carry scale 0), ds and
+    buffer_scales [nf, P]; chi, hardness, eta (and shift) [N] shared by the
+    frames or [nf, N]; the constraint C [n_const, N], b [n_const] holds in
+    every frame.  Returns q* [nf, N]; its gradients flow to positions, box,
+    chi, hardness, eta, ds and shift through the implicit adjoint (a second
+    batched CG with the same operator).  The reference solves one frame per
+    pgrad_optimize call (qeq.py:1117-1270)."""
+    nf, n = positions.shape[0], positions.shape[1]
+    dev, dt = positions.device, positions.dtype
+
+    def per_frame(v):
+        return v.reshape(-1, n).expand(nf, n) if v is not None else None
+
+    if q0 is None:
+        q0 = torch.zeros(nf, n, dtype=dt, device=dev)
+    if constraint_matrix is not None and constraint_vals is None:
+        constraint_vals = torch.zeros(constraint_matrix.shape[0], dtype=dt, device=dev)
+    if shift is None:
+        shift = torch.zeros(nf, n, dtype=dt, device=dev)
+    return QEqFramesFn.apply(positions, box, per_frame(chi), per_frame(hardness), per_frame(eta), ds,
+                             per_frame(shift), module, pairs, buffer_scales, constraint_matrix, constraint_vals,
+                             q0, module.eps if tol is None else tol, module.max_iter if max_iter is None else max_iter)

@@ -57,14 +57,9 @@ class AdmpPools(ctypes.Structure):
                [("mesh_cap", ctypes.c_longlong), ("spec", _P), ("spec_cap", ctypes.c_longlong), ("acc", _P),
                 ("acc_cap", ctypes.c_int), ("cells", _P), ("cells_cap", ctypes.c_longlong), ("sys_scratch", _P),
                 ("sys_scratch_bytes", ctypes.c_longlong), ("green", _P), ("green_cap", ctypes.c_longlong),
-                ("pos64", _P), ("box64", _P), ("frac64", _P), ("xkey", _P), ("xkey_stride", ctypes.c_int),
-                ("flags", ctypes.c_int)]
-
-SERVE_CLUSTER_MATVEC = 1
+                ("pos64", _P), ("box64", _P), ("frac64", _P), ("flags", ctypes.c_int)]
 
 _COPY_THREADS = 4  # host threads copying request arrays into the pinned staging buffers
-# ints per slot of the x-key tables (mesh planes along x + 1)
-XKEY_STRIDE = 1024
 
 
 def _bind_serve(lib):
@@ -168,8 +163,7 @@ class ServingEngine:
     def __init__(self, device="cuda:0", dtype=torch.float32, max_atoms: int = 4_000_000, max_slots: int = 512,
                  pairs_per_atom: float = 150.0, mesh_budget: int = 64_000_000, rcut: float = 6.0,
                  ethresh: float = 5e-4, tol: float = 1e-6, max_iter: int = 300, iters_per_tick: int = 8,
-                 ke: float = DIELECTRIC, green_budget: Optional[int] = None, admit_per_tick: int = 512,
-                 fused_recip: bool = False):
+                 ke: float = DIELECTRIC, green_budget: Optional[int] = None, admit_per_tick: int = 512):
         self.lib = L.load()
         _bind_serve(self.lib)
         self.dev = torch.device(device)
@@ -205,7 +199,6 @@ class ServingEngine:
             "sys_scratch": torch.zeros(self.lib.admp_serve_sys_scratch_bytes(MAX_PER_LAUNCH), dtype=torch.uint8,
                                        device=self.dev),
             "green": torch.zeros(green_budget if green_budget is not None else mesh_budget, **f),
-            "xkey": torch.zeros(max_slots * XKEY_STRIDE, **i32),
         }
         if dtype == torch.float32:
             # double copies for the neighbour decisions: the FP32 pair set equals the FP64 one
@@ -216,8 +209,7 @@ class ServingEngine:
         self.pools = AdmpPools()
         for name in ("pos", "q", "chi", "hardness", "eta", "force", "frac", "pstart", "pcnt", "cell_of", "sorted",
                      "col", "coef", "box", "energy", "cg_state", "slot_info", "cg_x", "cg_r", "cg_diag", "cg_z",
-                     "cg_chi", "cg_hx", "cg_p", "cg_hp", "mesh", "spec", "acc", "cells", "sys_scratch", "green",
-                     "xkey"):
+                     "cg_chi", "cg_hx", "cg_p", "cg_hp", "mesh", "spec", "acc", "cells", "sys_scratch", "green"):
             setattr(self.pools, name, t[name].data_ptr())
         for name in ("pos64", "box64", "frac64"):
             setattr(self.pools, name, t[name].data_ptr() if name in t else None)
@@ -227,12 +219,7 @@ class ServingEngine:
         self.pools.cells_cap = t["cells"].numel()
         self.pools.sys_scratch_bytes = t["sys_scratch"].numel()
         self.pools.green_cap = t["green"].numel()
-        self.pools.xkey_stride = XKEY_STRIDE
-        # CG matvecs: atom-parallel spread / gather around the FFT passes; fused_recip=True runs each
-        # matvec as one cluster-resident kernel per system instead (whole mesh in the shared memory
-        # of a 16-CTA cluster), measured slower on the serving stream (645 vs 194 ms of
-        # reciprocal work per 2000-request pass)
-        self.pools.flags = SERVE_CLUSTER_MATVEC if fused_recip else 0
+        self.pools.flags = 0
         self.greens = _Intervals(t["green"].numel(), 32)
         self.mesh_budget = mesh_budget
         self.atoms = _Intervals(A, 32)

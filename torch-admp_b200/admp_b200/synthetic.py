@@ -70,6 +70,16 @@ def water_system(n_mol: int, box_len: float, seed: int, jitter: float = 0.1,
     return pos, np.diag([box_len] * 3).astype(np.float64), chi, hard, eta, elem
 
 
+def water_frames(nframes: int, seed: int, n_mol: int = 1000, box_len: float = 31.0, jitter: float = 0.05):
+    """Frames of one water system (``water_system(n_mol, box_len, seed)``)
+    with every position jittered by N(0, jitter); frame f draws its jitter
+    from ``default_rng(seed + f)``.  Returns pos [nf, N, 3], box [nf, 3, 3],
+    chi, hardness, eta [N] (shared by the frames) and the element labels."""
+    pos0, box, chi, hard, eta, elem = water_system(n_mol, box_len, seed)
+    pos = np.stack([pos0 + np.random.default_rng(seed + f).normal(0.0, jitter, pos0.shape) for f in range(nframes)])
+    return pos, np.repeat(box[None], nframes, 0), chi, hard, eta, elem
+
+
 def electrode_system(seed: int, n_side: int = 24, n_layers: int = 2, a: float = 4.08,
                      gap: float = 40.0, n_ions: int = 3000, min_sep: float = 1.0,
                      slab_factor: float = 3.0):

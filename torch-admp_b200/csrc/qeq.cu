@@ -1,6 +1,8 @@
 // admp_qeq_solve / admp_qeq_hvp: matrix-free projected CG for the QEq and
 // electrode charges (replaces pgrad_optimize and the quadratic / LBFGS
 // minimisers, qeq.py:1117-1527, electrode.py:456-560).
+#include <vector>
+
 #include "pme_host.h"
 #include "qeq_kernels.cuh"
 
@@ -19,32 +21,38 @@ struct QEqWS {
   size_t bytes;
 };
 
+// nf frames of N atoms each (frame f: atoms [f N, (f+1) N), box f, mesh
+// kmesh[3 f .. 3 f + 2]); every per-atom vector spans all frames.
 template <typename T>
-static int qeq_carve(QEqWS<T>& w, void* ws, size_t bytes, int N, long long P, const int* kmesh, double kappa,
-                     int flags) {
-  SysSpec sys;
-  sys.natoms = N;
-  sys.atom_off = 0;
-  for (int d = 0; d < 3; ++d) sys.K[d] = (flags & ADMP_QEQ_KSPACE) ? kmesh[d] : 1;
-  sys.kappa = kappa > 0 ? kappa : 1.0;
-  sys.box_idx = 0;
-  int s = build_recip_plan<T>(&sys, 1, w.plan);
+static int qeq_carve(QEqWS<T>& w, void* ws, size_t bytes, int nf, int N, long long P, const int* kmesh,
+                     double kappa, int flags) {
+  if (nf <= 0 || nf > kMaxBatch) return fail(ADMP_ERR_BAD_ARG, "qeq: %d frames per call (1..%d)", nf, kMaxBatch);
+  SysSpec sys[kMaxBatch];
+  for (int f = 0; f < nf; ++f) {
+    sys[f].natoms = N;
+    sys[f].atom_off = f * N;
+    for (int d = 0; d < 3; ++d) sys[f].K[d] = (flags & ADMP_QEQ_KSPACE) ? kmesh[3 * f + d] : 1;
+    sys[f].kappa = kappa > 0 ? kappa : 1.0;
+    sys[f].box_idx = f;
+  }
+  int s = build_recip_plan<T>(sys, nf, w.plan);
   if (s) return s;
+  const size_t NT = (size_t)nf * N;
   Carver c(ws, bytes);
   w.mesh = c.take<T>((flags & ADMP_QEQ_KSPACE) ? w.plan.mesh_elems : 0);
   w.spec = c.take<Cplx<T>>((flags & ADMP_QEQ_KSPACE) ? w.plan.spec_elems : 0);
   w.green = c.take<T>((flags & ADMP_QEQ_KSPACE) ? w.plan.spec_elems : 0);
-  w.acc = c.take<double>(kAccStride);
-  w.x = c.take<double>(N);
-  w.r = c.take<double>(N);
-  w.diag = c.take<double>(N);
-  w.zc = c.take<double>(N);
-  w.chi_eff = c.take<double>(N);
-  w.hx = c.take<double>(N);
-  w.p = c.take<T>(N);
-  w.Hp = c.take<T>(N);
+  w.acc = c.take<double>((size_t)kAccStride * nf);
+  w.x = c.take<double>(NT);
+  w.r = c.take<double>(NT);
+  w.diag = c.take<double>(NT);
+  w.zc = c.take<double>(NT);
+  w.chi_eff = c.take<double>(NT);
+  w.hx = c.take<double>(NT);
+  w.p = c.take<T>(NT);
+  w.Hp = c.take<T>(NT);
   w.coef = c.take<T>(P > 0 ? P : 0);
-  w.sc = c.take<CGScal>(1);
+  w.sc = c.take<CGScal>(nf);
   w.bytes = c.off;
   return ADMP_OK;
 }
@@ -53,6 +61,7 @@ template <typename T>
 struct QEqCtx {
   QEqWS<T> w;
   QEqParams P;
+  int nf;
   int N;
   long long Pn;
   const long long* pairs;
@@ -76,7 +85,7 @@ static int qeq_matvec(QEqCtx<T>& c, const T* v, T* Hv, double* hv_out) {
   if (c.Pn > 0 && (c.P.flags & (ADMP_QEQ_RSPACE | ADMP_QEQ_DAMPING))) {
     long long blocks = (c.Pn + 255) / 256;
     if (blocks > 4096) blocks = 4096;
-    qeq_coo_spmv_kernel<T><<<(unsigned)blocks, 256, 0, c.st>>>(c.Pn, c.pairs, c.w.coef, v, Hv, c.w.sc);
+    qeq_coo_spmv_kernel<T><<<(unsigned)blocks, 256, 0, c.st>>>(c.Pn, c.pairs, c.w.coef, v, Hv, c.w.sc, c.N);
   }
   qeq_finish_kernel<T><<<b.nblk_atom, 256, 0, c.st>>>(b, c.P, v, Hv, c.w.diag, c.w.zc, c.C, (long long)c.N,
                                                      c.w.sc, hv_out);
@@ -88,8 +97,8 @@ template <typename T>
 static int qeq_prepare(QEqCtx<T>& c, const T* chi, const T* hard, const T* eta, const T* shift, const T* ds,
                        const T* bs, double kappa) {
   const Batch& b = c.w.plan.b;
-  ADMP_CUDA_TRY(cudaMemsetAsync(c.w.sc, 0, sizeof(CGScal), c.st));
-  ADMP_CUDA_TRY(cudaMemsetAsync(c.w.Hp, 0, sizeof(T) * c.N, c.st));
+  ADMP_CUDA_TRY(cudaMemsetAsync(c.w.sc, 0, sizeof(CGScal) * c.nf, c.st));
+  ADMP_CUDA_TRY(cudaMemsetAsync(c.w.Hp, 0, sizeof(T) * c.N * (size_t)c.nf, c.st));
   qeq_setup_kernel<T><<<b.nblk_atom, 256, 0, c.st>>>(b, c.P, c.pos, c.box, chi, hard, eta, shift, c.w.diag, c.w.zc,
                                                     c.w.chi_eff, c.w.sc);
   if (c.P.flags & ADMP_QEQ_KSPACE) {
@@ -98,27 +107,27 @@ static int qeq_prepare(QEqCtx<T>& c, const T* chi, const T* hard, const T* eta, 
   }
   if (c.nc > 0) {
     qeq_gram_kernel<T><<<b.nblk_atom, 256, 0, c.st>>>(b, c.nc, c.C, (long long)c.N, c.w.sc);
-    qeq_gram_invert_kernel<<<1, 32, 0, c.st>>>(b, c.nc, c.w.sc);
+    qeq_gram_invert_kernel<<<(c.nf + 31) / 32, 32, 0, c.st>>>(b, c.nc, c.w.sc);
   }
   if (c.Pn > 0 && (c.P.flags & (ADMP_QEQ_RSPACE | ADMP_QEQ_DAMPING))) {
     DevError* err = scratch_error(c.st);
     long long blocks = (c.Pn + 255) / 256;
     if (blocks > 4096) blocks = 4096;
-    qeq_pair_coef_kernel<T><<<(unsigned)blocks, 256, 0, c.st>>>(c.N, c.Pn, c.P.flags, kappa, c.P.ke, c.pairs, ds, bs,
-                                                                eta, c.w.coef, err);
+    qeq_pair_coef_kernel<T><<<(unsigned)blocks, 256, 0, c.st>>>(c.N * c.nf, c.Pn, c.P.flags, kappa, c.P.ke, c.pairs,
+                                                                ds, bs, eta, c.w.coef, err);
   }
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
 }
 
 template <typename T>
-static int qeq_solve_impl(int flags, int N, const int* kmesh, const T* pos, const T* box, long long Pn,
+static int qeq_solve_impl(int flags, int nf, int N, const int* kmesh, const T* pos, const T* box, long long Pn,
                           const long long* pairs, const T* ds, const T* bs, const T* chi, const T* hard, const T* eta,
                           const T* shift, double kappa, double ke, int nc, const T* C, const double* bvals, T* q,
                           double tol, int max_iter, int* iters, double* resid, void* ws, size_t bytes,
                           cudaStream_t st) {
   QEqCtx<T> c;
-  int s = qeq_carve<T>(c.w, ws, bytes, N, Pn, kmesh, kappa, flags);
+  int s = qeq_carve<T>(c.w, ws, bytes, nf, N, Pn, kmesh, kappa, flags);
   if (s) return s;
   if (!ws || c.w.bytes > bytes) return fail(ADMP_ERR_WORKSPACE, "qeq workspace: need %zu bytes, got %zu", c.w.bytes, bytes);
   c.P.flags = flags;
@@ -126,6 +135,7 @@ static int qeq_solve_impl(int flags, int N, const int* kmesh, const T* pos, cons
   c.P.max_iter = max_iter;
   c.P.tol = tol;
   c.P.ke = ke;
+  c.nf = nf;
   c.N = N;
   c.Pn = Pn;
   c.pairs = pairs;
@@ -135,44 +145,46 @@ static int qeq_solve_impl(int flags, int N, const int* kmesh, const T* pos, cons
   c.nc = nc;
   c.st = st;
   const Batch& b = c.w.plan.b;
+  const long long NT = (long long)nf * N;
+  const int sb = (nf + 63) / 64;
   s = qeq_prepare<T>(c, chi, hard, eta, shift, ds, bs, kappa);
   if (s) return s;
   double bv[4] = {0, 0, 0, 0};
   for (int k = 0; k < nc; ++k) bv[k] = bvals[k];
-  qeq_set_b_kernel<<<1, 1, 0, st>>>(c.w.sc, nc, bv[0], bv[1], bv[2], bv[3]);
+  qeq_set_b_kernel<<<sb, 64, 0, st>>>(nf, c.w.sc, nc, bv[0], bv[1], bv[2], bv[3]);
   // x0 (optionally projected onto C x = b)
-  const int cb = (int)((N + 255) / 256 < 2048 ? (N + 255) / 256 : 2048);
-  cast_kernel<T><<<cb > 0 ? cb : 1, 256, 0, st>>>(N, q, c.w.x);
+  const int cb = (int)((NT + 255) / 256 < 2048 ? (NT + 255) / 256 : 2048);
+  cast_kernel<T><<<cb > 0 ? cb : 1, 256, 0, st>>>(NT, q, c.w.x);
   if ((flags & ADMP_QEQ_PROJECT_Q0) && nc > 0) {
     qeq_sums_kernel<T, double><<<b.nblk_atom, 256, 0, st>>>(b, c.w.x, c.w.zc, C, (long long)N, nc, 1, c.w.sc, nullptr,
                                                             nullptr);
     qeq_project_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, c.w.x, C, (long long)N, c.w.sc);
-    ADMP_CUDA_TRY(cudaMemsetAsync(c.w.sc, 0, offsetof(CGScal, Ginv), st));
+    qeq_clear_acc_kernel<<<sb, 64, 0, st>>>(nf, c.w.sc);
   }
   // H x0 -> hx (double); the p buffer carries x0 in T for the matvec
   qeq_sums_kernel<T, double><<<b.nblk_atom, 256, 0, st>>>(b, c.w.x, c.w.zc, C, (long long)N, nc, 0, c.w.sc, c.w.Hp,
                                                           c.w.p);
   s = qeq_matvec<T>(c, c.w.p, c.w.Hp, c.w.hx);
   if (s) return s;
-  ADMP_CUDA_TRY(cudaMemsetAsync(c.w.sc, 0, offsetof(CGScal, Ginv), st));
-  ADMP_CUDA_TRY(cudaMemsetAsync(c.w.Hp, 0, sizeof(T) * N, st));
+  qeq_clear_acc_kernel<<<sb, 64, 0, st>>>(nf, c.w.sc);
+  ADMP_CUDA_TRY(cudaMemsetAsync(c.w.Hp, 0, sizeof(T) * NT, st));
   qeq_resid_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, c.w.hx, c.w.chi_eff, C, (long long)N, c.w.zc, c.w.r, c.w.p,
                                                    c.w.sc, 0);
   qeq_resid_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, c.w.hx, c.w.chi_eff, C, (long long)N, c.w.zc, c.w.r, c.w.p,
                                                    c.w.sc, 1);
-  qeq_init_done_kernel<<<1, 32, 0, st>>>(b, c.P, c.w.sc);
+  qeq_init_done_kernel<<<(nf + 31) / 32, 32, 0, st>>>(b, c.P, c.w.sc);
   ADMP_CUDA_TRY(cudaGetLastError());
-  // iterate; check the device flag every `chunk` iterations
+  // iterate; read the per-frame done flags every `chunk` iterations
   RecipPlan<T> pl = c.w.plan;
   pl.b.done = &c.w.sc->done;
   pl.b.done_stride = (int)(sizeof(CGScal) / sizeof(int));
   c.w.plan = pl;
   const int chunk = 8;
   int it = 0;
-  CGScal h;
+  std::vector<CGScal> h(nf);
   while (true) {
     for (int k = 0; k < chunk; ++k) {
-      qeq_rotate_kernel<<<1, 32, 0, st>>>(b, c.w.sc);
+      qeq_rotate_kernel<<<(nf + 31) / 32, 32, 0, st>>>(b, c.w.sc);
       s = qeq_matvec<T>(c, c.w.p, c.w.Hp, nullptr);
       if (s) return s;
       qeq_update_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, c.w.x, c.w.r, c.w.p, c.w.Hp, C, (long long)N, c.w.sc);
@@ -180,21 +192,31 @@ static int qeq_solve_impl(int flags, int N, const int* kmesh, const T* pos, cons
     }
     ADMP_CUDA_TRY(cudaGetLastError());
     it += chunk;
-    ADMP_CUDA_TRY(cudaMemcpyAsync(&h, c.w.sc, sizeof(CGScal), cudaMemcpyDeviceToHost, st));
+    ADMP_CUDA_TRY(cudaMemcpyAsync(h.data(), c.w.sc, sizeof(CGScal) * nf, cudaMemcpyDeviceToHost, st));
     ADMP_CUDA_TRY(cudaStreamSynchronize(st));
-    if (h.done || it > max_iter + chunk) break;
+    bool all = true;
+    for (int f = 0; f < nf; ++f) all = all && h[f].done;
+    if (all || it > max_iter + chunk) break;
   }
-  cast_back_kernel<T><<<cb > 0 ? cb : 1, 256, 0, st>>>(N, c.w.x, q);
+  cast_back_kernel<T><<<cb > 0 ? cb : 1, 256, 0, st>>>(NT, c.w.x, q);
   ADMP_CUDA_TRY(cudaGetLastError());
-  if (iters) *iters = h.iter;
-  if (resid) *resid = sqrt(h.rr_new > 0 ? h.rr_new : h.rr) / (N > 0 ? N : 1);
+  int worst = ADMP_OK, worst_f = 0;
+  for (int f = 0; f < nf; ++f) {
+    if (iters) iters[f] = h[f].iter;
+    if (resid) resid[f] = sqrt(h[f].rr_new > 0 ? h[f].rr_new : h[f].rr) / (N > 0 ? N : 1);
+    const int stf = h[f].done ? h[f].status : ADMP_ERR_NOT_CONVERGED;
+    if (stf && (worst == ADMP_OK || worst == ADMP_ERR_NOT_CONVERGED)) {
+      worst = stf;
+      worst_f = f;
+    }
+  }
   DevError* err = scratch_error(st);
   int e = err ? check_error(err, st) : ADMP_OK;
   if (e) return e;
-  if (h.status == ADMP_ERR_NOT_CONVERGED)
-    return fail(ADMP_ERR_NOT_CONVERGED, "QEq CG did not converge in %d iterations (residual %g)", h.iter,
-                resid ? *resid : 0.0);
-  if (h.status) return fail(h.status, "QEq solve failed (status %d)", h.status);
+  if (worst == ADMP_ERR_NOT_CONVERGED)
+    return fail(ADMP_ERR_NOT_CONVERGED, "QEq CG did not converge in %d iterations (frame %d, residual %g)",
+                h[worst_f].iter, worst_f, sqrt(h[worst_f].rr_new > 0 ? h[worst_f].rr_new : h[worst_f].rr) / N);
+  if (worst) return fail(worst, "QEq solve failed (frame %d, status %d)", worst_f, worst);
   return ADMP_OK;
 }
 
@@ -203,9 +225,10 @@ static int qeq_hvp_impl(int flags, int N, const int* kmesh, const T* pos, const 
                         const long long* pairs, const T* ds, const T* bs, const T* hard, const T* eta, double kappa,
                         double ke, const T* p, T* out, void* ws, size_t bytes, cudaStream_t st) {
   QEqCtx<T> c;
-  int s = qeq_carve<T>(c.w, ws, bytes, N, Pn, kmesh, kappa, flags);
+  int s = qeq_carve<T>(c.w, ws, bytes, 1, N, Pn, kmesh, kappa, flags);
   if (s) return s;
   if (!ws || c.w.bytes > bytes) return fail(ADMP_ERR_WORKSPACE, "qeq workspace: need %zu bytes, got %zu", c.w.bytes, bytes);
+  c.nf = 1;
   c.P.flags = flags;
   c.P.axis = (flags >> 8) & 3;
   c.P.max_iter = 0;
@@ -235,19 +258,62 @@ static int qeq_hvp_impl(int flags, int N, const int* kmesh, const T* pos, const 
 
 using namespace admp;
 
-extern "C" size_t admp_qeq_workspace_size(int dtype, int natoms, long long npairs, const int* kmesh, int n_const) {
-  (void)n_const;
-  int K[3] = {1, 1, 1};
+static size_t qeq_ws_bytes(int dtype, int nframes, int natoms, long long npairs, const int* kmesh) {
+  if (nframes <= 0 || nframes > kMaxBatch || natoms <= 0) return 0;
+  std::vector<int> K(3 * (size_t)nframes, 1);
   if (kmesh)
-    for (int d = 0; d < 3; ++d) K[d] = kmesh[d];
+    for (size_t k = 0; k < K.size(); ++k) K[k] = kmesh[k];
+  const int fl = kmesh ? ADMP_QEQ_KSPACE : 0;
   if (dtype == ADMP_F32) {
     QEqWS<float> w;
-    if (qeq_carve<float>(w, nullptr, 0, natoms, npairs, K, 1.0, kmesh ? ADMP_QEQ_KSPACE : 0)) return 0;
-    return w.bytes;
+    return qeq_carve<float>(w, nullptr, 0, nframes, natoms, npairs, K.data(), 1.0, fl) ? 0 : w.bytes;
   }
   QEqWS<double> w;
-  if (qeq_carve<double>(w, nullptr, 0, natoms, npairs, K, 1.0, kmesh ? ADMP_QEQ_KSPACE : 0)) return 0;
-  return w.bytes;
+  return qeq_carve<double>(w, nullptr, 0, nframes, natoms, npairs, K.data(), 1.0, fl) ? 0 : w.bytes;
+}
+
+extern "C" size_t admp_qeq_workspace_size(int dtype, int natoms, long long npairs, const int* kmesh, int n_const) {
+  (void)n_const;
+  return qeq_ws_bytes(dtype, 1, natoms, npairs, kmesh);
+}
+
+extern "C" size_t admp_qeq_frames_workspace_size(int dtype, int nframes, int natoms, long long npairs,
+                                                 const int* kmesh, int n_const) {
+  (void)n_const;
+  return qeq_ws_bytes(dtype, nframes, natoms, npairs, kmesh);
+}
+
+extern "C" int admp_qeq_solve_frames(int dtype, int flags, int nframes, int natoms, const int* kmesh, const void* pos,
+                                     const void* box, long long npairs, const long long* pairs, const void* ds,
+                                     const void* buffer_scales, const void* chi, const void* hardness,
+                                     const void* eta, const void* rhs_shift, double kappa, double ke, int n_const,
+                                     const void* C, const double* b, void* q, double tol, int max_iter, int* iters,
+                                     double* resid, void* workspace, size_t workspace_bytes, void* stream) {
+  if (nframes <= 0 || nframes > kMaxBatch)
+    return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: %d frames (1..%d)", nframes, kMaxBatch);
+  if (natoms <= 0 || !pos || !box || !hardness || !q) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: args");
+  if (n_const < 0 || n_const > kMaxConst || (n_const > 0 && (!C || !b)))
+    return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: n_const must be in [0, %d] with C and b", kMaxConst);
+  if ((flags & ADMP_QEQ_KSPACE) && (!kmesh || !(kappa > 0))) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: kspace needs kmesh and kappa");
+  if ((flags & ADMP_QEQ_DAMPING) && !eta) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: damping needs eta");
+  if (npairs > 0 && (!pairs || !ds || !buffer_scales)) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: pairs");
+  std::vector<int> K(3 * (size_t)nframes, 1);
+  if (flags & ADMP_QEQ_KSPACE)
+    for (size_t k = 0; k < K.size(); ++k) K[k] = kmesh[k];
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == ADMP_F64)
+    return qeq_solve_impl<double>(flags, nframes, natoms, K.data(), (const double*)pos, (const double*)box, npairs,
+                                  pairs, (const double*)ds, (const double*)buffer_scales, (const double*)chi,
+                                  (const double*)hardness, (const double*)eta, (const double*)rhs_shift, kappa, ke,
+                                  n_const, (const double*)C, b, (double*)q, tol, max_iter, iters, resid, workspace,
+                                  workspace_bytes, st);
+  if (dtype == ADMP_F32)
+    return qeq_solve_impl<float>(flags, nframes, natoms, K.data(), (const float*)pos, (const float*)box, npairs, pairs,
+                                 (const float*)ds, (const float*)buffer_scales, (const float*)chi,
+                                 (const float*)hardness, (const float*)eta, (const float*)rhs_shift, kappa, ke,
+                                 n_const, (const float*)C, b, (float*)q, tol, max_iter, iters, resid, workspace,
+                                 workspace_bytes, st);
+  return fail(ADMP_ERR_BAD_ARG, "bad dtype");
 }
 
 extern "C" int admp_qeq_solve(int dtype, int flags, int natoms, const int* kmesh, const void* pos, const void* box,
@@ -256,26 +322,9 @@ extern "C" int admp_qeq_solve(int dtype, int flags, int natoms, const int* kmesh
                               double kappa, double ke, int n_const, const void* C, const double* b, void* q,
                               double tol, int max_iter, int* iters, double* resid, void* workspace,
                               size_t workspace_bytes, void* stream) {
-  if (natoms <= 0 || !pos || !box || !hardness || !q) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: args");
-  if (n_const < 0 || n_const > kMaxConst || (n_const > 0 && (!C || !b)))
-    return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: n_const must be in [0, %d] with C and b", kMaxConst);
-  if ((flags & ADMP_QEQ_KSPACE) && (!kmesh || !(kappa > 0))) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: kspace needs kmesh and kappa");
-  if ((flags & ADMP_QEQ_DAMPING) && !eta) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: damping needs eta");
-  if (npairs > 0 && (!pairs || !ds || !buffer_scales)) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_solve: pairs");
-  cudaStream_t st = (cudaStream_t)stream;
-  if (dtype == ADMP_F64)
-    return qeq_solve_impl<double>(flags, natoms, kmesh, (const double*)pos, (const double*)box, npairs, pairs,
-                                  (const double*)ds, (const double*)buffer_scales, (const double*)chi,
-                                  (const double*)hardness, (const double*)eta, (const double*)rhs_shift, kappa, ke,
-                                  n_const, (const double*)C, b, (double*)q, tol, max_iter, iters, resid, workspace,
-                                  workspace_bytes, st);
-  if (dtype == ADMP_F32)
-    return qeq_solve_impl<float>(flags, natoms, kmesh, (const float*)pos, (const float*)box, npairs, pairs,
-                                 (const float*)ds, (const float*)buffer_scales, (const float*)chi,
-                                 (const float*)hardness, (const float*)eta, (const float*)rhs_shift, kappa, ke,
-                                 n_const, (const float*)C, b, (float*)q, tol, max_iter, iters, resid, workspace,
-                                 workspace_bytes, st);
-  return fail(ADMP_ERR_BAD_ARG, "bad dtype");
+  return admp_qeq_solve_frames(dtype, flags, 1, natoms, kmesh, pos, box, npairs, pairs, ds, buffer_scales, chi,
+                               hardness, eta, rhs_shift, kappa, ke, n_const, C, b, q, tol, max_iter, iters, resid,
+                               workspace, workspace_bytes, stream);
 }
 
 extern "C" int admp_qeq_hvp(int dtype, int flags, int natoms, const int* kmesh, const void* pos, const void* box,

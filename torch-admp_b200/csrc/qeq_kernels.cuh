@@ -50,8 +50,9 @@ __device__ __forceinline__ bool sys_done(const CGScal* sc, int s) {
   return sc[s].done != 0;
 }
 
-// Constraint row c at atom i; a null matrix stands for the single all-ones
-// row of the total-charge constraint.
+// Constraint row c at atom i of a system (i counts within the system, so the
+// frames of a multi-frame solve share one [n_const, N] matrix); a null matrix
+// stands for the single all-ones row of the total-charge constraint.
 template <typename T>
 __device__ __forceinline__ double cval(const T* C, int c, long long cstride, int i) {
   return C ? (double)C[(long long)c * cstride + i] : 1.0;
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(256)
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = d.atom_off + a;
     for (int r = 0; r < nc; ++r)
-      for (int c = 0; c < nc; ++c) v[r * kMaxConst + c] += cval(C, r, cstride, i) * cval(C, c, cstride, i);
+      for (int c = 0; c < nc; ++c) v[r * kMaxConst + c] += cval(C, r, cstride, i - d.atom_off) * cval(C, c, cstride, i - d.atom_off);
   }
   block_atomic_sum<16>(v, sc[s].Ginv, red);
 }
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(256)
     acc[1] += x * z;
     acc[2] += x * z * z;
     if (want_cv)
-      for (int c = 0; c < nc; ++c) acc[3 + c] += cval(C, c, cstride, i) * x;
+      for (int c = 0; c < nc; ++c) acc[3 + c] += cval(C, c, cstride, i - d.atom_off) * x;
     if (hv_zero) hv_zero[i] = T(0);
     if (vt) vt[i] = (T)x;
   }
@@ -211,16 +212,17 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Hv[i] += c_p v[j], Hv[j] += c_p v[i]  (single system, COO)
+// Hv[i] += c_p v[j], Hv[j] += c_p v[i]  (COO over the frames of a batch:
+// atom i belongs to frame i / natoms, whose CG state is sc[i / natoms])
 template <typename T>
 __global__ void __launch_bounds__(256)
     qeq_coo_spmv_kernel(long long Pn, const long long* __restrict__ pairs, const T* __restrict__ coef,
-                        const T* __restrict__ v, T* __restrict__ Hv, const CGScal* __restrict__ sc) {
-  if (sc[0].done) return;
+                        const T* __restrict__ v, T* __restrict__ Hv, const CGScal* __restrict__ sc, int natoms) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < Pn; p += (long long)gridDim.x * blockDim.x) {
     const T c = coef[p];
     if (c == T(0)) continue;
     const long long i = pairs[2 * p], j = pairs[2 * p + 1];
+    if (sc[i / natoms].done) continue;
     atomicAdd(Hv + i, c * v[j]);
     atomicAdd(Hv + j, c * v[i]);
   }
@@ -255,7 +257,7 @@ __global__ void __launch_bounds__(256)
     Hv[i] = (T)h;
     if (hv_out) hv_out[i] = h;
     acc[0] += x * h;
-    for (int c = 0; c < nc; ++c) acc[1 + c] += cval(C, c, cstride, i) * h;
+    for (int c = 0; c < nc; ++c) acc[1 + c] += cval(C, c, cstride, i - d.atom_off) * h;
   }
   double a1v[1] = {acc[0]};
   block_atomic_sum<1>(a1v, &sc[s].pHp, red);
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(256)
     const int i = d.atom_off + a;
     double w = (double)Hp[i];
     Hp[i] = T(0);
-    for (int c = 0; c < nc; ++c) w -= cval(C, c, cstride, i) * lam[c];
+    for (int c = 0; c < nc; ++c) w -= cval(C, c, cstride, i - d.atom_off) * lam[c];
     x[i] += alpha * (double)p[i];
     const double rn = r[i] - alpha * w;
     r[i] = rn;
@@ -370,7 +372,7 @@ __global__ void __launch_bounds__(256)
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = d.atom_off + a;
     double v = x[i];
-    for (int c = 0; c < nc; ++c) v += cval(C, c, cstride, i) * lam[c];
+    for (int c = 0; c < nc; ++c) v += cval(C, c, cstride, i - d.atom_off) * lam[c];
     x[i] = v;
   }
 }
@@ -394,7 +396,7 @@ __global__ void __launch_bounds__(256)
     for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
       const int i = d.atom_off + a;
       const double g = chi_eff[i] + hx[i];
-      for (int c = 0; c < nc; ++c) acc[c] += cval(C, c, cstride, i) * g;
+      for (int c = 0; c < nc; ++c) acc[c] += cval(C, c, cstride, i - d.atom_off) * g;
     }
     if (nc > 0) block_atomic_sum<4>(acc, sc[s].Cv, red);
     return;
@@ -406,7 +408,7 @@ __global__ void __launch_bounds__(256)
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = d.atom_off + a;
     double g = chi_eff[i] + hx[i];
-    for (int c = 0; c < nc; ++c) g -= cval(C, c, cstride, i) * lam[c];
+    for (int c = 0; c < nc; ++c) g -= cval(C, c, cstride, i - d.atom_off) * lam[c];
     const double rv = -g;
     r[i] = rv;
     p[i] = (T)rv;
@@ -422,15 +424,31 @@ __global__ void __launch_bounds__(256)
   block_atomic_sum<3>(a3, &sc[s].sp, red);
 }
 
-// After the initial residual: decide done, clear accumulators.
-static __global__ void qeq_set_b_kernel(CGScal* __restrict__ sc, int nc, double b0, double b1, double b2, double b3) {
-  if (threadIdx.x == 0) {
-    sc[0].b[0] = b0;
-    sc[0].b[1] = b1;
-    sc[0].b[2] = b2;
-    sc[0].b[3] = b3;
-    sc[0].n_const = nc;
-  }
+// Constraint values b (shared by every system of the batch) and their count.
+static __global__ void qeq_set_b_kernel(int nsys, CGScal* __restrict__ sc, int nc, double b0, double b1, double b2,
+                                        double b3) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  sc[s].b[0] = b0;
+  sc[s].b[1] = b1;
+  sc[s].b[2] = b2;
+  sc[s].b[3] = b3;
+  sc[s].n_const = nc;
+}
+
+// Zero the CG accumulators (rr .. spz2) of every system, keeping Ginv, b and
+// the per-system constants.
+static __global__ void qeq_clear_acc_kernel(int nsys, CGScal* __restrict__ sc) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  CGScal& S = sc[s];
+  S.rr = 0.0;
+  S.rr_new = 0.0;
+  S.pHp = 0.0;
+  for (int c = 0; c < kMaxConst; ++c) S.Cv[c] = 0.0;
+  S.sp = 0.0;
+  S.spz = 0.0;
+  S.spz2 = 0.0;
 }
 
 template <typename T>

@@ -2,13 +2,8 @@
 // with per-slot state (positions, CSR neighbour rows, CG vectors and scalars)
 // that persists in caller-owned pools between calls, so a scheduler can admit
 // and retire systems between CG iterations (continuous batching).
-#include <map>
-#include <mutex>
-#include <tuple>
-
 #include "pme_host.h"
 #include "qeq_kernels.cuh"
-#include "recip_cluster.cuh"
 #include "serve_kernels.cuh"
 
 namespace admp {
@@ -209,122 +204,6 @@ static int serve_ef_impl(const admp_pools* P, const admp_sys* sys, int nsys, dou
   return ADMP_OK;
 }
 
-// ---------------------------------------------------------------------------
-// Cluster-resident reciprocal matvec: per system the smallest cluster size
-// C in {1, 2, 4, 8, 16} whose CTAs hold the system's mesh in shared memory and
-// of which one cluster can be resident; systems grouped by C, one launch per
-// group.  Used only when every system of the batch qualifies.
-// ---------------------------------------------------------------------------
-struct ClusterPlan {
-  int ncls = 0;
-  ClusterList cls[10];
-  size_t smem[10];
-};
-
-constexpr size_t kClusterSmemLimit = 220 * 1024;
-
-template <typename T>
-static bool cluster_fits(int C, size_t smem) {
-  static std::mutex mu;
-  static std::map<std::tuple<int, int, size_t>, bool> cache;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  const size_t bucket = (smem + 8191) / 8192 * 8192;
-  const auto key = std::make_tuple(dev, C, bucket);
-  std::lock_guard<std::mutex> lock(mu);
-  auto it = cache.find(key);
-  if (it != cache.end()) return it->second;
-  bool ok = cudaFuncSetAttribute(recip_pot_cluster_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
-                cudaSuccess &&
-            ensure_smem(recip_pot_cluster_kernel<T>, kClusterSmemLimit) == cudaSuccess;
-  if (ok) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(C, 1, 1);
-    cfg.blockDim = dim3(kClusterThreads, 1, 1);
-    cfg.dynamicSmemBytes = bucket < kClusterSmemLimit ? bucket : kClusterSmemLimit;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = C;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    int n = 0;
-    ok = cudaOccupancyMaxActiveClusters(&n, recip_pot_cluster_kernel<T>, &cfg) == cudaSuccess && n > 0;
-  }
-  cudaGetLastError();  // an unsupported size is an answer, not an error
-  cache[key] = ok;
-  return ok;
-}
-
-template <typename T>
-static bool build_cluster_plan(const admp_pools* P, const RecipPlan<T>& rp, ClusterPlan& cp) {
-  cp.ncls = 0;
-  if (!(P->flags & ADMP_SERVE_CLUSTER_MATVEC) || !P->xkey || !P->green || P->xkey_stride <= 0) return false;
-  int pick[kMaxBatch];
-  size_t need[kMaxBatch];
-  for (int s = 0; s < rp.b.nsys; ++s) {
-    const SysDesc& d = rp.b.s[s];
-    if (d.K0 + 1 > P->xkey_stride) return false;
-    // as many CTAs as a cluster may have (few planes each, so one system's
-    // phases are short and a chunk of systems fills the GPU)
-    int C = kClusterMaxSize;
-    while (C > d.K0) C >>= 1;
-    const size_t sm = cluster_smem_bytes<T>(d.K0, d.K1, d.K2, C);
-    if (sm > kClusterSmemLimit || !cluster_fits<T>(C, sm)) return false;
-    pick[s] = sm <= kClusterSmemLimit / 2 ? C : -C;  // two launches by shared-memory size
-    need[s] = sm;
-  }
-  for (int k = 0; k < 10; ++k) {
-    const int C = (k & 1 ? -1 : 1) * (1 << (k >> 1));
-    ClusterList& L = cp.cls[cp.ncls];
-    L.n = 0;
-    L.C = C < 0 ? -C : C;
-    size_t sm = 0;
-    for (int s = 0; s < rp.b.nsys; ++s)
-      if (pick[s] == C) {
-        L.sys[L.n++] = s;
-        sm = sm > need[s] ? sm : need[s];
-      }
-    if (L.n) cp.smem[cp.ncls++] = sm;
-  }
-  return true;
-}
-
-template <typename T>
-static int launch_cluster_pot(const ClusterPlan& cp, const RecipPlan<T>& rp, const admp_pools* P, const T* v, T* pot,
-                              cudaStream_t st) {
-  const int h = prof_begin(st);
-  for (int k = 0; k < cp.ncls; ++k) {
-    const ClusterList& L = cp.cls[k];
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(L.n * L.C, 1, 1);
-    cfg.blockDim = dim3(kClusterThreads, 1, 1);
-    cfg.dynamicSmemBytes = cp.smem[k];
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = L.C;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    ADMP_CUDA_TRY(cudaLaunchKernelEx(&cfg, recip_pot_cluster_kernel<T>, rp.b, L, (const T*)P->pos, (const T*)P->box,
-                                     v, (const int*)P->sorted, (const int*)P->xkey, P->xkey_stride,
-                                     (const T*)P->green, pot));
-  }
-  // algorithmic DRAM bytes: positions, charges, order and potential per atom, the cached Green's function
-  double bytes = 0;
-  for (int s = 0; s < rp.b.nsys; ++s) {
-    const SysDesc& d = rp.b.s[s];
-    bytes += (double)d.natoms * (3 * sizeof(T) + 2 * sizeof(T) + sizeof(int)) +
-             (double)d.K0 * d.K1 * d.K2h * sizeof(T);
-  }
-  prof_end(h, PK_RECIP_FUSED, bytes, st);
-  count_launches(cp.ncls);
-  return ADMP_OK;
-}
-
 // CSR SpMV (QEq real-space matrix times v) fused with the end of the matvec (as
 // qeq_finish_kernel): per row h = (recip + J_real v)_i + diag_i v_i + nn sum(v)
 // (+ slab terms), Hv_i = h, and the block sums of v.h and C.h into the CG
@@ -411,11 +290,10 @@ static __global__ void __launch_bounds__(256)
 // H v for the listed systems: Hv must be zeroed, sums of v in the CG state.
 template <typename T>
 static int srv_matvec(const admp_pools* P, const RecipPlan<T>& plan, QEqParams prm, const T* v, T* Hv,
-                      double* hv_out, double ke, cudaStream_t st, const ClusterPlan* cp = nullptr) {
+                      double* hv_out, double ke, cudaStream_t st) {
   const Batch& b = plan.b;
-  int s = cp ? launch_cluster_pot<T>(*cp, plan, P, v, Hv, st)
-             : launch_recip_potential<T>(plan, (const T*)P->pos, (const T*)P->box, v, (T*)P->mesh,
-                                         (Cplx<T>*)P->spec, P->acc, ke, Hv, st, P->sorted, (const T*)P->green);
+  int s = launch_recip_potential<T>(plan, (const T*)P->pos, (const T*)P->box, v, (T*)P->mesh, (Cplx<T>*)P->spec,
+                                    P->acc, ke, Hv, st, P->sorted, (const T*)P->green);
   if (s) return s;
   int h = prof_begin(st);
   csr_spmv_finish_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, P->pstart, P->pcnt, P->col, (const T*)P->coef, v,
@@ -468,21 +346,10 @@ static int serve_qeq_init_impl(const admp_pools* P, const admp_sys* sys, int nsy
                                                           nullptr, nullptr);
   qeq_project_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_x, (const T*)nullptr, 0, sc);
   slot_clear_acc_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc);
-  // atoms sorted by x plane key for the cluster-resident matvec (positions are fixed during the solve);
-  // every slot with K0 + 1 <= xkey_stride is sorted, so any later batch of them may take the cluster path
-  ClusterPlan cp;
-  const bool use_cluster = build_cluster_plan<T>(P, plan, cp);
-  if ((P->flags & ADMP_SERVE_CLUSTER_MATVEC) && P->xkey && P->green && P->xkey_stride > 0) {
-    int mk = 1;
-    for (int k = 0; k < nsys; ++k) mk = mk > b.s[k].K0 ? mk : b.s[k].K0;
-    xkey_sort_kernel<T><<<nsys, 1024, (mk + 1) * sizeof(int), st>>>(b, (const T*)P->pos, (const T*)P->box,
-                                                                     P->sorted, P->xkey, P->xkey_stride);
-    count_launches(1);
-  }
   // H x0
   qeq_sums_kernel<T, double><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_x, P->cg_z, (const T*)nullptr, 0, 1, 0, sc,
                                                           (T*)P->cg_hp, (T*)P->cg_p);
-  s = srv_matvec<T>(P, plan, prm, (const T*)P->cg_p, (T*)P->cg_hp, P->cg_hx, ke, st, use_cluster ? &cp : nullptr);
+  s = srv_matvec<T>(P, plan, prm, (const T*)P->cg_p, (T*)P->cg_hp, P->cg_hx, ke, st);
   if (s) return s;
   slot_clear_acc_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc);
   zero_vec_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, (T*)P->cg_hp);
@@ -509,12 +376,10 @@ static int serve_qeq_iterate_impl(const admp_pools* P, const admp_sys* sys, int 
   plan.b.done_stride = (int)(sizeof(CGScal) / sizeof(int));
   const Batch& b = plan.b;
   const QEqParams prm = srv_params(tol, max_iter, ke);
-  ClusterPlan cp;
-  const bool use_cluster = build_cluster_plan<T>(P, plan, cp);
   for (int k = 0; k < niter; ++k) {
     count_launches(3);
     qeq_rotate_kernel<<<(nsys + 31) / 32, 32, 0, st>>>(b, sc);
-    s = srv_matvec<T>(P, plan, prm, (const T*)P->cg_p, (T*)P->cg_hp, nullptr, ke, st, use_cluster ? &cp : nullptr);
+    s = srv_matvec<T>(P, plan, prm, (const T*)P->cg_p, (T*)P->cg_hp, nullptr, ke, st);
     if (s) return s;
     const int hv = prof_begin(st);
     qeq_update_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_x, P->cg_r, (const T*)P->cg_p, (T*)P->cg_hp,

@@ -65,9 +65,12 @@ def parse():
     ap.add_argument("--nreq", type=int, default=N_REQ)
     ap.add_argument("--latency-rate", type=float, default=LAT_RATE,
                     help="open-loop Poisson arrival rate (requests/s) for p50/p99")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-reps", type=int, default=None,
+                    help="repetitions of the CPU sample (default 3 for --impl reference, 1 beside the GPU arm)")
     ap.add_argument("--plain-sample", type=int, default=100)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the FP64 serving, electrode and differentiation-batch legs")
     ap.add_argument("--timeline", action="store_true",
                     help="after the timed passes, trace one device-resident pass call by call (CUDA events "
                          "around each library call) and print the accounting as JSON on stderr")
@@ -101,7 +104,8 @@ def rank_stream(nreq: int, rank: int):
 def _cpu_one(req_tuple):
     """One request on the CPU oracle (restatement of the reference path:
     cell-list neighbours, PME energy + forces, or the reference's projected
-    nonlinear CG for QEq followed by energy + forces).  Returns seconds."""
+    nonlinear CG for QEq followed by energy + forces).  Returns (seconds,
+    energy, forces, charges or None)."""
     from oracle import admp_oracle as O
     t0 = time.perf_counter()
     kind, pos, box, q, chi, hard, eta = req_tuple
@@ -110,54 +114,84 @@ def _cpu_one(req_tuple):
     pairs = O.nblist_pbc_cells(pos, box, RCUT)
     bs = O.pair_buffer_scales(pairs)
     if kind == "pme":
-        O.coulomb_forces(pos, box, pairs, bs, q, rcut=RCUT, ethresh=ETHRESH, kmesh=km)
-        return time.perf_counter() - t0
+        o = O.coulomb_forces(pos, box, pairs, bs, q, rcut=RCUT, ethresh=ETHRESH, kmesh=km)
+        return time.perf_counter() - t0, o["E"], o["forces"], None
     ds = O.pairs_ds(pos, pairs, box)
     s = O.QEqSystem(pos, box, chi, hard, eta, pairs, ds, bs, rcut=RCUT, ethresh=ETHRESH, kmesh=km)
     n = pos.shape[0]
     qs, _ = O.solve_quadratic(s, np.zeros(n), np.ones((1, n)), np.zeros(1), max_iter=200, eps=TOL)
-    O.coulomb_forces(pos, box, pairs, bs, qs, rcut=RCUT, ethresh=ETHRESH, kmesh=km)
-    return time.perf_counter() - t0
+    E, _ = s.energy_grad(qs)
+    o = O.coulomb_forces(pos, box, pairs, bs, qs, rcut=RCUT, ethresh=ETHRESH, kmesh=km)
+    _, dds, _, _ = O.damping(qs, eta, pairs, ds, bs)
+    dpd, _ = O.ds_backward(pos, box, pairs, dds)
+    return time.perf_counter() - t0, E, o["forces"] - dpd, qs
 
 
-CPU_SAMPLE_SIZES = {"pme": (300, 1000, 3000, 6000), "qeq": (300, 900, 2400)}
+CPU_SAMPLE = 48   # requests of the size-stratified CPU sample
 
 
-def cpu_baseline(stream, seconds: float):
-    """CPU oracle throughput on the stream, from a timed sample.
+def cpu_sample(stream, k: int = CPU_SAMPLE):
+    """k requests of the stream, one from each of k equal-count strata of the
+    stream sorted by atom count (the request at each stratum's middle), so
+    the sample follows the stream's size distribution and mix of kinds."""
+    srt = sorted(stream, key=lambda r: (r.natoms, r.rid))
+    n = len(srt)
+    return [srt[min(n - 1, int((j + 0.5) * n / k))] for j in range(min(k, n))]
 
-    Requests of each kind closest to the sizes in CPU_SAMPLE_SIZES are run
-    one per process on the host cores (spawn pool); a power law t = a N^b
-    fitted per kind to their single-core times predicts every request of the
-    stream, and the stream throughput is cores / mean(predicted time) (the
-    requests are independent, so they spread over the cores).  Returns
-    (systems/s, cores, sample text)."""
+
+def cpu_baseline(stream, reps: int = 1):
+    """CPU oracle throughput, measured: the size-stratified sample of the
+    stream runs on every host core at once (spawn pool, one request per
+    task, largest first), timed by the wall clock; value = sample requests /
+    wall seconds, the median over `reps` repetitions.  Also returns the
+    per-request core-seconds, from which a secondary figure extrapolates
+    per kind (power law in N) to the whole stream.  Returns (systems/s,
+    cores, description, details dict)."""
     import multiprocessing as mp
     cores = os.cpu_count() or 1
-    picks = []
-    for kind, sizes in CPU_SAMPLE_SIZES.items():
-        cand = [r for r in stream if r.kind == kind]
-        for n in sizes:
-            if cand:
-                picks.append(min(cand, key=lambda r: abs(r.natoms - n)))
-    tasks = [(r.kind, r.pos, r.box, r.charges, r.chi, r.hardness, r.eta) for r in picks]
+    picks = cpu_sample(stream)
+    order = sorted(range(len(picks)), key=lambda j: -(picks[j].natoms * (8 if picks[j].kind == "qeq" else 1)))
+    tasks = [(picks[j].kind, picks[j].pos, picks[j].box, picks[j].charges, picks[j].chi, picks[j].hardness,
+              picks[j].eta) for j in order]
     ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
+    walls, times, outs = [], None, None
     with ctx.Pool(min(cores, len(tasks))) as pool:
-        times = pool.map(_cpu_one, tasks, chunksize=1)
-    wall = time.perf_counter() - t0
+        pool.map(_cpu_warm, range(min(cores, len(tasks))), chunksize=1)
+        for _ in range(max(1, reps)):
+            t0 = time.perf_counter()
+            outs = pool.map(_cpu_one, tasks, chunksize=1)
+            walls.append(time.perf_counter() - t0)
+            t = [o[0] for o in outs]
+            times = t if times is None else [min(a, b) for a, b in zip(times, t)]
+    wall = statistics.median(walls)
+    value = len(tasks) / wall
+    # secondary: power law t = a N^b per kind over the measured requests, summed over the whole stream
+    byreq = [(picks[j], tt) for j, tt in zip(order, times)]
     pred = 0.0
-    for kind in CPU_SAMPLE_SIZES:
-        pts = [(r.natoms, t) for r, t in zip(picks, times) if r.kind == kind]
-        x = np.log([p[0] for p in pts])
-        y = np.log([p[1] for p in pts])
+    for kind in ("pme", "qeq"):
+        pts = [(r.natoms, tt) for r, tt in byreq if r.kind == kind]
+        if not pts:
+            continue
+        x = np.log([p_[0] for p_ in pts])
+        y = np.log([p_[1] for p_ in pts])
         b, a = np.polyfit(x, y, 1) if len(pts) > 1 else (1.0, y[0] - x[0])
         pred += sum(math.exp(a + b * math.log(r.natoms)) for r in stream if r.kind == kind)
-    value = cores * len(stream) / pred
-    desc = (f"{len(picks)} requests timed single-core ({', '.join(f'{r.kind} {r.natoms}: {t:.2f}s' for r, t in zip(picks, times))}; "
-            f"wall {wall:.1f}s), power-law fit per kind extrapolated to all {len(stream)} requests "
-            f"(predicted {pred:.0f} core-seconds)")
-    return value, cores, desc
+    nq = sum(1 for r in picks if r.kind == "qeq")
+    desc = (f"{len(tasks)} requests ({len(tasks) - nq} PME, {nq} QEq; {min(r.natoms for r in picks)}-"
+            f"{max(r.natoms for r in picks)} atoms, one per atom-count stratum of the stream) on {cores} cores at "
+            f"once, wall {wall:.1f} s (median of {len(walls)}: {', '.join(f'{w:.1f}' for w in walls)}), "
+            f"{sum(times):.0f} core-seconds")
+    details = {"wall_s": walls, "core_seconds": sum(times), "requests": len(tasks),
+               "extrapolated_stream_value": cores * len(stream) / pred if pred > 0 else None,
+               "rids": [r.rid for r in picks],
+               "results": {picks[j].rid: o[1:] for j, o in zip(order, outs)}}
+    return value, cores, desc, details
+
+
+def _cpu_warm(_):
+    """Import the oracle in a pool worker before the timed repetitions."""
+    from oracle import admp_oracle  # noqa: F401
+    return 0
 
 
 # ---------------------------------------------------------------- GPU helpers
@@ -279,6 +313,174 @@ def plain_path(stream, dev, dtype, n, eps=TOL):
     return len(sample) / (time.perf_counter() - t0), out
 
 
+def accuracy_vs(results, ref):
+    """Largest relative force error (per request, by its largest force) and
+    charge error (e) of serving results against reference (E, F, q) tuples."""
+    ferr = {"pme": 0.0, "qeq": 0.0}
+    qerr = 0.0
+    eerr = 0.0
+    for rid, (E, F, q) in ref.items():
+        o = results[rid]
+        k = "qeq" if q is not None else "pme"
+        ferr[k] = max(ferr[k], float(np.abs(np.asarray(o.forces, np.float64) - F).max() / np.abs(F).max()))
+        eerr = max(eerr, abs(o.energy - E) / abs(E))
+        if q is not None:
+            qerr = max(qerr, float(np.abs(np.asarray(o.charges, np.float64) - q).max()))
+    return {"max_rel_force_err": max(ferr.values()), "max_rel_force_err_pme": ferr["pme"],
+            "max_rel_force_err_qeq": ferr["qeq"], "max_charge_err_e": qerr, "max_rel_energy_err": eerr,
+            "requests": len(ref)}
+
+
+def same_sample_gpu(eng, reqs, passes: int = 3):
+    """The FP32 serving engine on the CPU baseline's sample (host numpy in and
+    out, as e2e): systems/s over `passes` passes after one untimed pass, and
+    the results of the last pass."""
+    import torch
+    eng.results_to_host = True
+    eng.results = []
+    eng.run(reqs, arrivals=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(passes):
+        eng.results = []
+        res = eng.run(reqs, arrivals=False)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / passes
+    return {"value": len(reqs) / dt, "unit": UNIT, "requests": len(reqs), "ms_per_pass": dt * 1e3,
+            "results": {r.rid: r for r in res}}
+
+
+def fp64_serving(stream, dev, args, world):
+    """The serving engine in FP64 arithmetic (the reference's precision) on
+    the same stream: device-resident and host-input (e2e) systems/s."""
+    import torch
+
+    from admp_b200.serving import ServingEngine, auto_kmesh
+    dstream = to_device_requests(stream, dev, torch.float64)
+    kap = math.sqrt(-math.log(2 * ETHRESH)) / RCUT
+    mesh_sum = sum(int(np.prod(auto_kmesh(np.diagonal(r.box), kap, ETHRESH))) for r in stream)
+    total_atoms = sum(r.natoms for r in stream)
+    eng = ServingEngine(device=dev, dtype=torch.float64, max_atoms=min(6_000_000, int(total_atoms * 1.1) + 65536),
+                        max_slots=min(1024, len(stream) + 8), mesh_budget=min(64_000_000, mesh_sum + 4_000_000),
+                        rcut=RCUT, ethresh=ETHRESH, tol=TOL, max_iter=300, iters_per_tick=8)
+    out = {}
+    for name, reqs, host in (("value", dstream, False), ("e2e", stream, True)):
+        eng.results_to_host = host
+        for _ in range(2):
+            eng.results = []
+            eng.run(reqs, arrivals=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        passes = max(1, min(args.steps, 3))
+        for _ in range(passes):
+            eng.results = []
+            res = eng.run(reqs, arrivals=False)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / passes
+        out[name] = len(reqs) * world / max_over_ranks(dt, dev)
+        out[f"{name}_failed"] = sum(1 for r in res if r.status != 0)
+    del eng
+    torch.cuda.empty_cache()
+    return {"value": out["value"], "e2e": out["e2e"], "unit": UNIT, "dtype": "f64",
+            "failed_requests": out["value_failed"] + out["e2e_failed"],
+            "note": "device-resident and host-input passes of the same stream, FP64 bulk arithmetic"}
+
+
+def electrode_leg(dev):
+    """Constant-potential electrodes at their stated size (2 x 1,152 fcc(111)
+    electrode atoms at 1 V / 0 V, 3,000 ions, 64 x 64 x 160 mesh, slab
+    correction): GPU time of infer() (neighbour list, electrode solve, energy
+    and forces) in FP32 and FP64, and the errors against the reference's
+    result for the same system (tests/golden/electrode_cfg3.npz)."""
+    import torch
+
+    from admp_b200 import synthetic
+    from admp_b200.electrode import LAMMPSElectrodeConstraint, PolarizableElectrode, infer, setup_from_lammps
+    from admp_b200.nblist import TorchNeighborList
+    pos_np, box_np, q_np, top, bot = synthetic.electrode_system(SEED)
+    gpath = os.path.join(ROOT, "tests", "golden", "electrode_cfg3.npz")
+    g = np.load(gpath) if os.path.exists(gpath) else None
+    out = {"electrode_atoms": int(len(top) + len(bot)), "atoms": int(len(q_np)), "kmesh": [64, 64, 160]}
+    for dt, eps, tag in ((torch.float32, 1e-7, "fp32"), (torch.float64, 1e-10, "fp64")):
+        calc = PolarizableElectrode(rcut=RCUT, ethresh=ETHRESH, kmesh=[64, 64, 160], slab_corr=True, eps=eps,
+                                    max_iter=2000)
+        cons = [LAMMPSElectrodeConstraint(indices=top, value=1.0, mode="conp", eta=math.sqrt(2.0)),
+                LAMMPSElectrodeConstraint(indices=bot, value=0.0, mode="conp", eta=math.sqrt(2.0))]
+
+        def run():
+            pos = torch.tensor(pos_np, dtype=dt, device=dev, requires_grad=True)
+            box = torch.tensor(box_np, dtype=dt, device=dev)
+            ch = torch.tensor(q_np, dtype=dt, device=dev)
+            nb = TorchNeighborList(RCUT)
+            pairs = nb(pos, box)
+            data = setup_from_lammps(len(q_np), cons, True, device=dev, dtype=dt)
+            E, F, q = infer(calc, pos, box, ch, pairs, nb.get_ds(), nb.get_buffer_scales(), *data, method="lbfgs")
+            return float(E), F.detach().double().cpu().numpy(), q.detach().double().cpu().numpy()
+
+        run()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            E, F, q = run()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        r = {"ms": statistics.median(ts) * 1e3, "cg_iterations": calc.converge_iter}
+        if g is not None:
+            r["max_rel_force_err_vs_reference"] = float(np.abs(F - g["forces"]).max() / np.abs(g["forces"]).max())
+            r["max_charge_err_vs_reference_e"] = float(np.abs(q - g["q_ref"]).max())
+            r["rel_energy_err_vs_reference"] = abs(E - float(g["E"])) / abs(float(g["E"]))
+        out[tag] = r
+    if g is not None:
+        out["reference_cpu_s"] = float(g["time_ref_s"])
+        out["reference_cpu_note"] = (f"the reference's infer(method='lbfgs', eps 1e-8) on {int(g['threads'])} CPU "
+                                     "threads, timed when the golden file was made (not on this host)")
+    return out
+
+
+def diff_batch_leg(dev, nframes: int = 64):
+    """The differentiation batch: 64 jittered frames of the 3,000-atom water
+    system (48^3 mesh), neighbour lists + batched charge solve + energy +
+    gradients w.r.t. positions, box, chi, hardness and eta through the
+    implicit adjoint, in FP32 and FP64 (median of 3 after one warm-up)."""
+    import torch
+
+    from admp_b200 import synthetic
+    from admp_b200.nblist import frame_pair_lists
+    from admp_b200.qeq import QEqForceModule, qeq_solve_frames
+    pos_np, box_np, chi_np, hard_np, eta_np, _ = synthetic.water_frames(nframes, SEED)
+    out = {"frames": nframes, "atoms_per_frame": int(pos_np.shape[1])}
+    for dt, tol, tag in ((torch.float32, 1e-7, "fp32"), (torch.float64, 1e-10, "fp64")):
+        m = QEqForceModule(RCUT, ETHRESH, kmesh=48, eps=tol, max_iter=1000)
+
+        def run():
+            pos = torch.tensor(pos_np, dtype=dt, device=dev, requires_grad=True)
+            box = torch.tensor(box_np, dtype=dt, device=dev, requires_grad=True)
+            chi = torch.tensor(chi_np, dtype=dt, device=dev, requires_grad=True)
+            hard = torch.tensor(hard_np, dtype=dt, device=dev, requires_grad=True)
+            eta = torch.tensor(eta_np, dtype=dt, device=dev, requires_grad=True)
+            pairs, ds, bs = frame_pair_lists(pos, box, RCUT)
+            n = pos.shape[1]
+            C = torch.ones(1, n, dtype=dt, device=dev)
+            q = qeq_solve_frames(m, pos, box, chi, hard, eta, pairs, ds, bs, C, tol=tol)
+            params = {"charge": q, "chi": chi.expand(nframes, n), "hardness": hard.expand(nframes, n),
+                      "eta": eta.expand(nframes, n)}
+            E = m(pos, box, pairs, ds, bs, params)
+            return torch.autograd.grad(E.sum(), [pos, box, chi, hard, eta])
+
+        run()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            run()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        ms = statistics.median(ts) * 1e3
+        out[tag] = {"ms": ms, "frames_per_s": nframes / (ms / 1e3), "max_cg_iterations": m.converge_iter}
+    return out
+
+
 def main():
     args = parse()
     rank, world, local = rank_info()
@@ -287,18 +489,14 @@ def main():
         if rank != 0:
             return
         stream = synthetic.serving_stream(args.nreq, SEED, RATE)
-        vals = []
-        for _ in range(max(args.steps, 1)):
-            v, cores, sample = cpu_baseline(stream, max(args.cpu_seconds, 5.0))
-            vals.append(v)
-        v = statistics.median(vals)
+        v, cores, sample, det = cpu_baseline(stream, args.cpu_reps or 3)
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": f"serving stream, {args.nreq} requests (200-20000 atoms, 60% PME / 40% QEq)",
                            "rcut": RCUT, "ethresh": ETHRESH, "cg_tol": TOL},
-                "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                                 "sample": sample + " per step"},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                                 "extrapolated_stream_value": det["extrapolated_stream_value"]},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -454,10 +652,21 @@ def main():
     achieved = rf[dom]["gbs"]
     alg_per_launch = achieved * 1e9 * rf[dom]["ms_per_launch"] / 1e3
     traffic = TRAFFIC_PER_ALG_BYTE[dom] * alg_per_launch if dom in TRAFFIC_PER_ALG_BYTE else None
+    extra = {}
+    if not args.no_extra:
+        extra["fp64"] = fp64_serving(stream, dev, args, world)
+        extra["electrode_cfg3"] = electrode_leg(dev)
+        extra["diff_batch_cfg4"] = diff_batch_leg(dev)
     cpu = None
+    same = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, cores, sample = cpu_baseline(stream, args.cpu_seconds)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        sample_reqs = cpu_sample(stream)
+        same = same_sample_gpu(eng, sample_reqs)
+        v, cores, sample, det = cpu_baseline(stream, args.cpu_reps or 1)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+               "extrapolated_stream_value": det["extrapolated_stream_value"]}
+        same["cpu_value"] = v
+        same["accuracy_vs_oracle"] = accuracy_vs(same.pop("results"), det["results"])
     clocks = clk.summary(t_clk0, t_clk1)
     if rank == 0:
         line = {
@@ -492,6 +701,8 @@ def main():
         }
         if cpu:
             line["cpu_baseline"] = cpu
+            line["same_sample"] = same
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -107,8 +107,13 @@ int admp_pme_recip(int dtype, int nframes, int natoms, const int* kmesh, const v
 /* by every GPU that loads the library until exit; calls needing more       */
 /* scratch than that (admp_pme_recip_workspace_size) return               */
 /* ADMP_ERR_WORKSPACE.  The first call on a device looks up the array's     */
-/* device address (cudaGetSymbolAddress) and should come before any stream */
-/* capture.  All calls share the array: calls that overlap on the GPU race. */
+/* device address (cudaGetSymbolAddress); with CUDA's lazy module loading   */
+/* that first lookup also loads the library's module, which is when the    */
+/* array itself is created (a device allocation that may synchronise).  So  */
+/* make one call (or a warm-up call) per device before the region that must */
+/* not allocate, and before any stream capture.  The looked-up address is   */
+/* cached per device and is not valid after cudaDeviceReset.  All calls     */
+/* share the array: calls that overlap on the GPU race.                     */
 size_t admp_pme_recip_noalloc_max_scratch(void);
 int admp_pme_recip_noalloc(int dtype, int nframes, int natoms, const int* kmesh, const void* pos,
                            const void* box, const void* q, double kappa, double ke, double* energy,
@@ -255,6 +260,19 @@ int admp_qeq_hvp(int dtype, int flags, int natoms, const int* kmesh, const void*
                  double ke, const void* p, void* out, void* workspace, size_t workspace_bytes,
                  void* stream);
 
+/* admp_qeq_hvp for nframes frames at once (the layout of                     */
+/* admp_qeq_solve_frames; workspace from admp_qeq_frames_workspace_size):    */
+/* out [nframes, N] = H_f p_f.  The dense Hessian of matinv_optimize /       */
+/* calc_hessian (qeq.py:460-515, 1620-1670) is built from these, one batch   */
+/* of unit vectors (frames of the same geometry) per call, instead of one    */
+/* autograd pass per column.                                                 */
+int admp_qeq_hvp_frames(int dtype, int flags, int nframes, int natoms, const int* kmesh,
+                        const void* pos, const void* box, long long npairs,
+                        const long long* pairs, const void* ds, const void* buffer_scales,
+                        const void* hardness, const void* eta, double kappa, double ke,
+                        const void* p, void* out, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Batched serving.  Many independent systems (PME energy+forces requests or */
 /* QEq solves) run per launch; their state lives in caller-owned pools so a   */
@@ -325,6 +343,13 @@ typedef struct admp_pools {
   double* box64;       /* [S,3,3] or NULL */
   void* frac64;        /* [A] double4 scratch, needed with pos64 */
   int flags;           /* reserved, 0 */
+  /* optional per-slot cell tables written by admp_serve_neighbors: cells per
+   * axis, a valid flag, then the start of each cell's atoms in `sorted`
+   * (cells + 1 entries); with them the reciprocal-space spread and gather
+   * work on bricks of cells in shared memory.  NULL: the direct kernels.    */
+  int* celltab;        /* [S, celltab_stride] */
+  int celltab_stride;  /* ints per slot (>= 5 + cells of the largest system) */
+  double* slot_resid;  /* optional [S]: ||P grad||_2 / N of each QEq slot's latest iterate */
 } admp_pools;
 
 size_t admp_serve_slot_state_bytes(void);

@@ -64,6 +64,25 @@ def test_noalloc_matches_workspace_entry_point_twice(cuda, dtype, tol):
             assert err < tol, err
 
 
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-11), (torch.float32, 2e-5)])
+def test_noalloc_smaller_mesh_after_larger_one(cuda, dtype, tol):
+    """A call with a different, smaller mesh layout right after the two-frame
+    call: whatever the previous call left in the shared array must not leak
+    into it (compared with the workspace entry point on a fresh workspace)."""
+    from admp_b200 import _lib as L
+    lib = L.load()
+    dt = L.dtype_code(dtype)
+    pos, box, q = _inputs(cuda, dtype)
+    _call(lib, lib.admp_pme_recip_noalloc, dt, pos, box, q, [[24, 24, 24], [24, 25, 23]], False)
+    p1, b1, q1 = _inputs(cuda, dtype, n=200, L=15.0, nf=1, seed=5)
+    kmesh = [[18, 17, 20]]
+    ref = _call(lib, lib.admp_pme_recip, dt, p1, b1, q1, kmesh, True)
+    out = _call(lib, lib.admp_pme_recip_noalloc, dt, p1, b1, q1, kmesh, False)
+    for a, b in zip(out, ref):
+        err = (a - b).abs().max().item() / max(b.abs().max().item(), 1e-30)
+        assert err < tol, err
+
+
 def test_noalloc_rejects_scratch_beyond_its_limit(cuda):
     from admp_b200 import _lib as L
     lib = L.load()

@@ -42,7 +42,7 @@ EXPORTS = [
     "admp_check_errors", "admp_pme_recip_workspace_size", "admp_pme_recip", "admp_pair_energy",
     "admp_atom_terms", "admp_pair_distances", "admp_pair_distances_backward", "admp_nblist_workspace_size",
     "admp_nblist_count", "admp_nblist_fill", "admp_qeq_workspace_size", "admp_qeq_solve", "admp_qeq_hvp",
-    "admp_qeq_frames_workspace_size", "admp_qeq_solve_frames",
+    "admp_qeq_frames_workspace_size", "admp_qeq_solve_frames", "admp_qeq_hvp_frames",
     "admp_launch_count", "admp_profile_enable", "admp_profile_read", "admp_serve_slot_state_bytes",
     "admp_serve_sys_scratch_bytes", "admp_serve_cells_needed", "admp_serve_neighbors", "admp_serve_energy_forces",
     "admp_serve_qeq_init", "admp_serve_qeq_iterate", "admp_serve_qeq_finish", "admp_pme_recip_noalloc_max_scratch",
@@ -79,6 +79,8 @@ _SIGS = {
     "admp_qeq_frames_workspace_size": (_sz, [_i, _i, _i, _ll, _ip, _i]),
     "admp_qeq_solve_frames": (_i, [_i, _i, _i, _i, _ip, _vp, _vp, _ll, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d,
                                    _i, _vp, _dp, _vp, _d, _i, _ip, _dp, _vp, _sz, _vp]),
+    "admp_qeq_hvp_frames": (_i, [_i, _i, _i, _i, _ip, _vp, _vp, _ll, _vp, _vp, _vp, _vp, _vp, _d, _d, _vp, _vp,
+                                 _vp, _sz, _vp]),
     "admp_qeq_hvp": (_i, [_i, _i, _i, _ip, _vp, _vp, _ll, _vp, _vp, _vp, _vp, _vp, _d, _d, _vp, _vp, _vp, _sz,
                           _vp]),
     "admp_launch_count": (_ll, []),

@@ -252,38 +252,50 @@ def _qeq_solve_raw(module, q0, positions, box, chi, hardness, eta, pairs, ds, bu
     return q, int(iters.value), float(resid.value), st
 
 
-def _hvp(module, pos, bx, pr, dsc, bsc, hard_c, eta_c, v):
+def _hessian(module, positions, box, hardness, eta, pairs, ds, buffer_scales, max_cols: int = 64,
+             max_pair_rows: int = 16_000_000):
+    """Dense d2E/dq2 from batched GPU Hessian-vector products: columns in
+    chunks, each chunk one admp_qeq_hvp_frames call on unit vectors (the
+    geometry repeated per column), with one workspace for all chunks."""
     lib = L.load()
-    n = pos.shape[0]
-    dt = pos.dtype
-    c = module.submodels["coulomb"]
-    km = _kmesh_of(module, bx)
-    kp, _keep = L.int3(km)
-    flags = module._flags()
-    nbytes = lib.admp_qeq_workspace_size(L.dtype_code(dt), n, pr.shape[0], kp if c.kspace_flag else None, 0)
-    ws = L.workspace(nbytes, pos.device)
-    out = torch.empty_like(v)
-    L.check(lib.admp_qeq_hvp(L.dtype_code(dt), flags, n, kp, L.ptr(pos), L.ptr(bx), pr.shape[0], L.ptr(pr),
-                             L.ptr(dsc), L.ptr(bsc), L.ptr(hard_c), L.ptr(eta_c), float(c.kappa) or 1.0,
-                             module.const_lib.dielectric, L.ptr(v), L.ptr(out), L.ptr(ws), nbytes,
-                             L.stream_of(pos.device)), "QEq Hessian-vector product")
-    return out
-
-
-def _hessian(module, positions, box, hardness, eta, pairs, ds, buffer_scales):
     ec = module.const_lib.energy_coeff
     pos, bx, pr, dsc, bsc, (hard_c, eta_c) = _std_inputs(
         module, positions, box, pairs, ds, buffer_scales, hardness * ec,
         eta * module.const_lib.length_coeff if eta is not None else None)
     n = pos.shape[0]
+    dt, dev = pos.dtype, pos.device
     if eta_c is None:
-        eta_c = torch.zeros(n, dtype=pos.dtype, device=pos.device)
-    H = torch.empty(n, n, dtype=pos.dtype, device=pos.device)
-    e = torch.zeros(n, dtype=pos.dtype, device=pos.device)
-    for k in range(n):
-        e.zero_()
-        e[k] = 1.0
-        H[:, k] = _hvp(module, pos, bx, pr, dsc, bsc, hard_c, eta_c, e)
+        eta_c = torch.zeros(n, dtype=dt, device=dev)
+    P = int(pr.shape[0])
+    nv = max(1, min(max_cols, n, max_pair_rows // max(P, 1)))
+    c = module.submodels["coulomb"]
+    km = _kmesh_of(module, bx)
+    flags = module._flags()
+    kp, _keep = L.int3(km * nv)
+    nbytes = lib.admp_qeq_frames_workspace_size(L.dtype_code(dt), nv, n, P * nv, kp if c.kspace_flag else None, 0)
+    if nbytes == 0:
+        L.check(L.BAD_ARG, "QEq Hessian workspace")
+    ws = L.workspace(nbytes, dev)
+    offs = (torch.arange(nv, device=dev, dtype=torch.long) * n).view(nv, 1, 1)
+    pos_r = pos.reshape(1, n, 3).expand(nv, n, 3).contiguous()
+    box_r = bx.reshape(1, 3, 3).expand(nv, 3, 3).contiguous()
+    pr_r = (pr.reshape(1, P, 2) + offs).reshape(-1, 2).contiguous()
+    ds_r = dsc.reshape(1, P).expand(nv, P).contiguous()
+    bs_r = bsc.reshape(1, P).expand(nv, P).contiguous()
+    hard_r = hard_c.reshape(1, n).expand(nv, n).contiguous()
+    eta_r = eta_c.reshape(1, n).expand(nv, n).contiguous()
+    H = torch.empty(n, n, dtype=dt, device=dev)
+    E = torch.zeros(nv, n, dtype=dt, device=dev)
+    out = torch.empty(nv, n, dtype=dt, device=dev)
+    for k0 in range(0, n, nv):
+        m = min(nv, n - k0)
+        E.zero_()
+        E[torch.arange(m, device=dev), torch.arange(k0, k0 + m, device=dev)] = 1.0
+        L.check(lib.admp_qeq_hvp_frames(L.dtype_code(dt), flags, m, n, kp, L.ptr(pos_r), L.ptr(box_r), P * m,
+                                        L.ptr(pr_r), L.ptr(ds_r), L.ptr(bs_r), L.ptr(hard_r), L.ptr(eta_r),
+                                        float(c.kappa) or 1.0, module.const_lib.dielectric, L.ptr(E), L.ptr(out),
+                                        L.ptr(ws), nbytes, L.stream_of(dev)), "QEq Hessian-vector products")
+        H[:, k0:k0 + m] = out[:m].T
     return 0.5 * (H + H.T)
 
 

@@ -57,7 +57,11 @@ class AdmpPools(ctypes.Structure):
                [("mesh_cap", ctypes.c_longlong), ("spec", _P), ("spec_cap", ctypes.c_longlong), ("acc", _P),
                 ("acc_cap", ctypes.c_int), ("cells", _P), ("cells_cap", ctypes.c_longlong), ("sys_scratch", _P),
                 ("sys_scratch_bytes", ctypes.c_longlong), ("green", _P), ("green_cap", ctypes.c_longlong),
-                ("pos64", _P), ("box64", _P), ("frac64", _P), ("flags", ctypes.c_int)]
+                ("pos64", _P), ("box64", _P), ("frac64", _P), ("flags", ctypes.c_int), ("celltab", _P),
+                ("celltab_stride", ctypes.c_int), ("slot_resid", _P)]
+
+# ints per slot of the cell tables (header + cell starts; systems with more cells use the direct kernels)
+CELLTAB_STRIDE = 1024
 
 _COPY_THREADS = 4  # host threads copying request arrays into the pinned staging buffers
 
@@ -132,6 +136,7 @@ class Result:
     status: int
     t_arrival: float
     t_done: float
+    residual: float = 0.0   # QEq: final ||P grad||_2 / N of the charge solve (the reference's criterion)
 
     @property
     def latency(self) -> float:
@@ -163,7 +168,8 @@ class ServingEngine:
     def __init__(self, device="cuda:0", dtype=torch.float32, max_atoms: int = 4_000_000, max_slots: int = 512,
                  pairs_per_atom: float = 150.0, mesh_budget: int = 64_000_000, rcut: float = 6.0,
                  ethresh: float = 5e-4, tol: float = 1e-6, max_iter: int = 300, iters_per_tick: int = 8,
-                 ke: float = DIELECTRIC, green_budget: Optional[int] = None, admit_per_tick: int = 512):
+                 ke: float = DIELECTRIC, green_budget: Optional[int] = None, admit_per_tick: int = 512,
+                 bricks: bool = True):
         self.lib = L.load()
         _bind_serve(self.lib)
         self.dev = torch.device(device)
@@ -199,6 +205,8 @@ class ServingEngine:
             "sys_scratch": torch.zeros(self.lib.admp_serve_sys_scratch_bytes(MAX_PER_LAUNCH), dtype=torch.uint8,
                                        device=self.dev),
             "green": torch.zeros(green_budget if green_budget is not None else mesh_budget, **f),
+            "celltab": torch.zeros(max_slots * CELLTAB_STRIDE, **i32),
+            "slot_resid": torch.zeros(max_slots, **f64),
         }
         if dtype == torch.float32:
             # double copies for the neighbour decisions: the FP32 pair set equals the FP64 one
@@ -220,6 +228,11 @@ class ServingEngine:
         self.pools.sys_scratch_bytes = t["sys_scratch"].numel()
         self.pools.green_cap = t["green"].numel()
         self.pools.flags = 0
+        # reciprocal-space spread / gather on bricks of neighbour cells in shared memory (the cell tables
+        # come from the neighbour build); bricks=False keeps the atom-parallel kernels with global atomics
+        self.pools.celltab = t["celltab"].data_ptr() if bricks else None
+        self.pools.celltab_stride = CELLTAB_STRIDE
+        self.pools.slot_resid = t["slot_resid"].data_ptr()
         self.greens = _Intervals(t["green"].numel(), 32)
         self.mesh_budget = mesh_budget
         self.atoms = _Intervals(A, 32)
@@ -599,19 +612,24 @@ class ServingEngine:
         E.copy_(t["energy"], non_blocking=True)
         info = torch.empty(self.max_slots, 4, dtype=torch.int32, pin_memory=True)
         info.copy_(t["slot_info"], non_blocking=True)
+        resid = None
+        if qitems:
+            resid = torch.empty(self.max_slots, dtype=torch.float64, pin_memory=True)
+            resid.copy_(t["slot_resid"], non_blocking=True)
         ev = torch.cuda.Event()
         ev.record(self.stream)
-        return ("finish", ev, items, runs, qruns, F_all, q_all, E, info)
+        return ("finish", ev, items, runs, qruns, F_all, q_all, E, info, resid)
 
     def _complete_finish(self, rec, now_fn) -> None:
         """Results of a finish record out, resources freed (its event has passed)."""
-        _, _, items, runs, qruns, F_all, q_all, E, info = rec
+        _, _, items, runs, qruns, F_all, q_all, E, info, resid = rec
         host = self.results_to_host
         tdone = now_fn()
         Fsrc = F_all.numpy() if host else F_all
         qsrc = (q_all.numpy() if host else q_all) if q_all is not None else None
         Eh = E.numpy()
         ih = info.numpy()
+        rh = resid.numpy() if resid is not None else None
         # row of each system inside the gathered arrays (runs keep their alignment padding)
         off, qoff = {}, {}
         o = 0
@@ -643,7 +661,9 @@ class ServingEngine:
                 self.stats["d2h_bytes"] += n * 3 * Fsrc.itemsize + 8 + (n * qsrc.itemsize if qo is not None else 0)
             if qo is not None and a.req.meta and a.req.meta.get("system_id") is not None:
                 self.warm[a.req.meta["system_id"]] = qo.copy() if host else qo.clone()
-            self.results.append(Result(a.req.rid, a.req.kind, float(Eh[a.slot]), Fo, qo, it, st, a.t_arrival, tdone))
+            res = float(rh[a.slot]) if (rh is not None and a.kind == SYS_QEQ) else 0.0
+            self.results.append(Result(a.req.rid, a.req.kind, float(Eh[a.slot]), Fo, qo, it, st, a.t_arrival, tdone,
+                                       res))
             self._release(a)
 
     def _complete_iterate(self, rec) -> None:
@@ -701,7 +721,15 @@ class ServingEngine:
         per-slot done flags); results of earlier steps are read afterwards,
         so the device stays busy while the host schedules.  While arrived
         requests wait, this step's launches are left in flight even with no
-        CG batch running, so the next step's admission overlaps them."""
+        CG batch running, so the next step's admission overlaps them.
+
+        Every copy and launch goes to the engine's stream (the stream that
+        was current when the engine was built), whatever stream is current
+        at the call, so the staging-buffer events cover the uploads."""
+        with torch.cuda.stream(self.stream):
+            return self._tick(now_fn)
+
+    def _tick(self, now_fn) -> int:
         n0 = len(self.results)
         r0 = len(self._inflight)
         now = now_fn()
@@ -745,8 +773,12 @@ class ServingEngine:
         t0 = time.perf_counter()
         for r in requests:
             self.submit(r, t0 + (r.arrival * time_scale if arrivals else 0.0))
+        with torch.cuda.stream(self.stream):
+            return self._run_loop(t0, max_seconds)
+
+    def _run_loop(self, t0: float, max_seconds: float):
         while self.pending():
-            if self.tick() == 0 and not self.active_qeq and not self._inflight:
+            if self._tick(time.perf_counter) == 0 and not self.active_qeq and not self._inflight:
                 # nothing on the device: wait for the next arrival
                 nxt = min(t for _, t in self.queue) if self.queue else None
                 if nxt is not None:

@@ -13,6 +13,10 @@
 //
 // The array is a file-scope __device__ variable: every GPU that loads the
 // library holds kNoAllocScratchBytes (16 MiB) of it until the process exits.
+// Under CUDA's lazy module loading the module, and with it the array, is
+// created on a device by the first call there (its cudaGetSymbolAddress), so
+// that first call does allocate: callers make it before their no-allocation
+// region.  The address cached per device is not valid after cudaDeviceReset.
 // Requests whose scratch does not fit are rejected with ADMP_ERR_WORKSPACE.
 // All calls share the array and it keeps the previous call's contents; the
 // code clears what must start at zero (mesh and accumulators) on every call.

@@ -3,6 +3,7 @@
 
 #include <vector>
 
+#include "brick_kernels.cuh"
 #include "pme_kernels.cuh"
 #include "runtime.h"
 
@@ -17,20 +18,48 @@ struct SysSpec {
   long long green_off = -1;  // cached Green's function offset; -1: same as the spectrum offset
 };
 
-// Launch geometry of a batch.
+// Launch geometry of a batch.  hs is the host copy of the per-system table;
+// bind_plan uploads it and points b.s at the device copy.
 template <typename T>
 struct RecipPlan {
   Batch b;
+  SysDesc hs[kMaxBatch];
   size_t mesh_elems = 0;  // real mesh elements (all systems)
   size_t spec_elems = 0;  // complex spectrum elements
   size_t smem_z = 0, smem_y = 0, smem_x = 0;
-  // fused slab passes: one block per x plane (blk_slab offsets), when a plane fits
+  // fused slab passes: a block per run of x planes (blk_slab offsets), when a plane fits
   bool slab = false;
   int buf_elems = 0;
   size_t smem_slab = 0;
-  int nblk_slab = 0;
-  int blk_slab[kMaxBatch];
 };
+
+// The per-system table as one by-value parameter: the only launch of a call
+// that carries it.
+struct SysTable {
+  SysDesc s[kMaxBatch];
+};
+
+static __global__ void sys_table_kernel(SysTable t, int n, SysDesc* __restrict__ dst) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = t.s[i];
+}
+
+// Upload the plan's system table to `dev` (kMaxBatch entries of device
+// memory owned by the caller's workspace or pools) on stream `st`; the
+// launches that follow on the same stream read it through b.s.
+template <typename T>
+inline int bind_plan(RecipPlan<T>& p, SysDesc* dev, cudaStream_t st) {
+  if (!dev) return fail(ADMP_ERR_WORKSPACE, "no device memory for the system table");
+  SysTable t;
+  for (int s = 0; s < p.b.nsys; ++s) t.s[s] = p.hs[s];
+  sys_table_kernel<<<1, 128, 0, st>>>(t, p.b.nsys, dev);
+  count_launches(1);
+  ADMP_CUDA_TRY(cudaGetLastError());
+  p.b.s = dev;
+  return ADMP_OK;
+}
+
+// device bytes of a system table (kept 256-byte aligned for what follows it)
+inline size_t sys_table_bytes() { return align_up(sizeof(SysDesc) * kMaxBatch, 256); }
 
 template <typename T>
 inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
@@ -40,6 +69,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   b.apb = 256;
   b.done = nullptr;
   b.done_stride = 0;
+  b.s = nullptr;
   int maxK[3] = {1, 1, 1};
   for (int s = 0; s < nsys; ++s)
     for (int d = 0; d < 3; ++d) {
@@ -69,7 +99,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   int ba = 0, bz = 0, by = 0, bx = 0;
   size_t mo = 0, so = 0;
   for (int s = 0; s < nsys; ++s) {
-    SysDesc& d = b.s[s];
+    SysDesc& d = p.hs[s];
     d.atom_off = sys[s].atom_off;
     d.natoms = sys[s].natoms;
     d.K0 = sys[s].K[0];
@@ -111,11 +141,11 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   p.buf_elems = be;
   p.smem_slab = (2 * (size_t)be + maxK[1] + maxK[2]) * cs;
   p.slab = p.smem_slab <= 200 * 1024;
-  p.nblk_slab = 0;
+  b.nblk_slab = 0;
   for (int s = 0; s < nsys; ++s) {
-    p.blk_slab[s] = p.nblk_slab;
+    p.hs[s].blk_slab = b.nblk_slab;
     const int ppb = slab_ppb(be, slab_plane_elems(sys[s].K[1], sys[s].K[2]), sys[s].K[0]);
-    p.nblk_slab += (sys[s].K[0] + ppb - 1) / ppb;
+    b.nblk_slab += (sys[s].K[0] + ppb - 1) / ppb;
   }
   return ADMP_OK;
 }
@@ -143,15 +173,11 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
   // algorithmic bytes: z passes read/write M reals + Mh complex, y/x passes Mh complex in and out
   const double rb = (double)p.mesh_elems * sizeof(T), cb = (double)p.spec_elems * sizeof(Cplx<T>);
   int h;
-  Batch bs;  // slab launches: F_Y block offsets remapped to one block per x plane
   if (p.slab) {
-    bs = b;
-    for (int s = 0; s < b.nsys; ++s) bs.s[s].blk_y = p.blk_slab[s];
-    bs.nblk_y = p.nblk_slab;
     ADMP_CUDA_TRY(ensure_smem(fft_slab_fwd_kernel<T>, p.smem_slab));
     ADMP_CUDA_TRY(ensure_smem(fft_slab_inv_kernel<T>, p.smem_slab));
     h = prof_begin(st);
-    if (bs.nblk_y) fft_slab_fwd_kernel<T><<<bs.nblk_y, 256, p.smem_slab, st>>>(bs, mesh, spec, p.buf_elems);
+    if (b.nblk_slab) fft_slab_fwd_kernel<T><<<b.nblk_slab, 256, p.smem_slab, st>>>(b, mesh, spec, p.buf_elems);
     prof_end(h, PK_FFT_Z_FWD, rb + cb, st);
   } else {
     h = prof_begin(st);
@@ -172,7 +198,7 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
   prof_end(h, PK_FFT_X_GREEN, 2 * cb + (green ? (double)p.spec_elems * sizeof(T) : 0.0), st);
   if (p.slab) {
     h = prof_begin(st);
-    if (bs.nblk_y) fft_slab_inv_kernel<T><<<bs.nblk_y, 256, p.smem_slab, st>>>(bs, spec, mesh, p.buf_elems);
+    if (b.nblk_slab) fft_slab_inv_kernel<T><<<b.nblk_slab, 256, p.smem_slab, st>>>(b, spec, mesh, p.buf_elems);
     prof_end(h, PK_FFT_Z_INV, rb + cb, st);
     count_launches(3);
   } else {
@@ -202,29 +228,62 @@ inline size_t gather_smem() {
 template <typename T>
 inline double plan_atoms(const RecipPlan<T>& p) {
   double n = 0;
-  for (int s = 0; s < p.b.nsys; ++s) n += p.b.s[s].natoms;
+  for (int s = 0; s < p.b.nsys; ++s) n += p.hs[s].natoms;
   return n;
+}
+
+// Atoms binned in cells (order = the cell-sorted atoms, cells = the per-slot
+// cell tables) take the brick-privatised spread / gather; otherwise the
+// direct kernels.
+template <typename T>
+inline int launch_spread(const Batch& b, const T* pos, const T* box, const T* q, T* mesh, const int* order,
+                         const int* cells, int cell_stride, cudaStream_t st) {
+  if (!b.nblk_atom) return ADMP_OK;
+  if (cells && order) {
+    ADMP_CUDA_TRY(ensure_smem(spread_brick_kernel<T>, brick_smem<T, false>()));
+    spread_brick_kernel<T><<<b.nblk_atom, 256, brick_smem<T, false>(), st>>>(b, pos, box, q, mesh, order, cells,
+                                                                            cell_stride);
+  } else {
+    ADMP_CUDA_TRY(ensure_smem(spread_kernel<T>, spread_smem<T>()));
+    spread_kernel<T><<<b.nblk_atom, 256, spread_smem<T>(), st>>>(b, pos, box, q, mesh, order);
+  }
+  return ADMP_OK;
+}
+
+template <typename T, bool F>
+inline int launch_gather(const Batch& b, const T* pos, const T* box, const T* q, const T* phi, T* dE_dq,
+                         T* dE_dpos, double* acc, const int* order, const int* cells, int cell_stride,
+                         cudaStream_t st) {
+  if (!b.nblk_atom) return ADMP_OK;
+  if (cells && order) {
+    ADMP_CUDA_TRY(ensure_smem(gather_brick_kernel<T, F>, brick_smem<T, F>()));
+    gather_brick_kernel<T, F><<<b.nblk_atom, 256, brick_smem<T, F>(), st>>>(b, pos, box, q, phi, dE_dq, dE_dpos, acc,
+                                                                           T(1), order, cells, cell_stride);
+  } else {
+    ADMP_CUDA_TRY(ensure_smem(gather_kernel<T, F>, gather_smem<T, F>()));
+    gather_kernel<T, F><<<b.nblk_atom, 256, gather_smem<T, F>(), st>>>(b, pos, box, q, phi, dE_dq, dE_dpos, acc,
+                                                                       T(1), order);
+  }
+  return ADMP_OK;
 }
 
 template <typename T>
 inline int launch_recip(const RecipPlan<T>& p, const T* pos, const T* box, const T* q, T* mesh, Cplx<T>* spec,
                         double* acc, double ke, T* dE_dq, T* dE_dpos, cudaStream_t st,
-                        const int* order = nullptr) {
+                        const int* order = nullptr, const int* cells = nullptr, int cell_stride = 0) {
   const Batch& b = p.b;
   const double na = plan_atoms(p), mb = (double)p.mesh_elems * sizeof(T);
   ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
   int h = prof_begin(st);
-  ADMP_CUDA_TRY(ensure_smem(spread_kernel<T>, spread_smem<T>()));
-  ADMP_CUDA_TRY(ensure_smem(gather_kernel<T, true>, gather_smem<T, true>()));
-  if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, spread_smem<T>(), st>>>(b, pos, box, q, mesh, order);
+  int s = launch_spread<T>(b, pos, box, q, mesh, order, cells, cell_stride, st);
+  if (s) return s;
   prof_end(h, PK_SPREAD, na * 4 * sizeof(T) + mb, st);
   count_launches(1);
-  int s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st);
+  s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st);
   if (s) return s;
   h = prof_begin(st);
-  if (b.nblk_atom)
-    gather_kernel<T, true><<<b.nblk_atom, 256, gather_smem<T, true>(), st>>>(b, pos, box, q, mesh, dE_dq, dE_dpos,
-                                                                             acc, T(1), order);
+  s = launch_gather<T, true>(b, pos, box, q, mesh, dE_dq, dE_dpos, acc, order, cells, cell_stride, st);
+  if (s) return s;
   prof_end(h, PK_GATHER, mb + na * 4 * sizeof(T) + na * 3 * sizeof(T), st);
   count_launches(1);
   ADMP_CUDA_TRY(cudaGetLastError());
@@ -235,21 +294,20 @@ inline int launch_recip(const RecipPlan<T>& p, const T* pos, const T* box, const
 template <typename T>
 inline int launch_recip_potential(const RecipPlan<T>& p, const T* pos, const T* box, const T* v, T* mesh,
                                   Cplx<T>* spec, double* acc, double ke, T* pot, cudaStream_t st,
-                                  const int* order = nullptr, const T* green = nullptr) {
+                                  const int* order = nullptr, const T* green = nullptr, const int* cells = nullptr,
+                                  int cell_stride = 0) {
   const Batch& b = p.b;
   const double na = plan_atoms(p), mb = (double)p.mesh_elems * sizeof(T);
   ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
   int h = prof_begin(st);
-  ADMP_CUDA_TRY(ensure_smem(spread_kernel<T>, spread_smem<T>()));
-  ADMP_CUDA_TRY(ensure_smem(gather_kernel<T, false>, gather_smem<T, false>()));
-  if (b.nblk_atom) spread_kernel<T><<<b.nblk_atom, 256, spread_smem<T>(), st>>>(b, pos, box, v, mesh, order);
+  int s = launch_spread<T>(b, pos, box, v, mesh, order, cells, cell_stride, st);
+  if (s) return s;
   prof_end(h, PK_SPREAD, na * 4 * sizeof(T) + mb, st);
-  int s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st, green);
+  s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st, green);
   if (s) return s;
   h = prof_begin(st);
-  if (b.nblk_atom)
-    gather_kernel<T, false><<<b.nblk_atom, 256, gather_smem<T, false>(), st>>>(b, pos, box, v, mesh, pot, nullptr,
-                                                                               acc, T(1), order);
+  s = launch_gather<T, false>(b, pos, box, v, mesh, pot, nullptr, acc, order, cells, cell_stride, st);
+  if (s) return s;
   prof_end(h, PK_GATHER, mb + na * 4 * sizeof(T) + na * sizeof(T), st);
   count_launches(2);
   ADMP_CUDA_TRY(cudaGetLastError());

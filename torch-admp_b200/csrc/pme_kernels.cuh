@@ -21,7 +21,7 @@ namespace admp {
 struct SysDesc {
   int32_t atom_off, natoms;
   int32_t K0, K1, K2, K2h;
-  int32_t blk_atom, blk_z, blk_y, blk_x;
+  int32_t blk_atom, blk_z, blk_y, blk_x, blk_slab;
   int64_t mesh_off, spec_off;
   int64_t green_off;  // cached 2 G_s (half-spectrum layout) for CG matvecs
   double kappa;
@@ -29,16 +29,20 @@ struct SysDesc {
   int32_t flags;
 };
 
+// Launch descriptor, passed by value (a few dozen bytes): block counts and
+// tile sizes of the launch plus a pointer to the per-system table, which
+// lives in device memory (uploaded once per library call, so the launches
+// of a call do not each carry the whole table as a kernel parameter).
 struct Batch {
   int nsys;
-  int nblk_atom, nblk_z, nblk_y, nblk_x;
+  int nblk_atom, nblk_z, nblk_y, nblk_x, nblk_slab;
   int apb;  // atoms per block (atom kernels)
   int lp;   // line pairs per block (z passes)
   int zb;   // columns per block (y / x passes)
   int maxK0, maxK1, maxK2;
   const int* done;   // optional per-slot skip flags (done[slot * done_stride], slot = box_idx)
   int done_stride;
-  SysDesc s[kMaxBatch];
+  const SysDesc* s;  // device table [nsys]
 };
 
 __device__ __forceinline__ bool skip_sys(const Batch& b, int s) {
@@ -52,11 +56,11 @@ constexpr int kAccVk = 1;       // 9: dE/dB (B = box^-1) through k vectors
 constexpr int kAccWf = 10;      // 9: dE/dB through fractional coordinates
 constexpr int kAccSlots = 19;
 
-enum SysField { F_ATOM = 0, F_Z = 1, F_Y = 2, F_X = 3 };
+enum SysField { F_ATOM = 0, F_Z = 1, F_Y = 2, F_X = 3, F_SLAB = 4 };
 
 template <int F>
 __device__ __forceinline__ int blk_of(const SysDesc& d) {
-  return F == F_ATOM ? d.blk_atom : F == F_Z ? d.blk_z : F == F_Y ? d.blk_y : d.blk_x;
+  return F == F_ATOM ? d.blk_atom : F == F_Z ? d.blk_z : F == F_Y ? d.blk_y : F == F_X ? d.blk_x : d.blk_slab;
 }
 
 template <int F>
@@ -503,13 +507,13 @@ template <typename T>
 __global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __restrict__ mesh,
                                                            Cplx<T>* __restrict__ spec, int buf_elems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int s = find_sys<F_Y>(b, blockIdx.x);  // F_Y blocks are remapped to runs of x planes
+  const int s = find_sys<F_SLAB>(b, blockIdx.x);  // a block per run of x planes
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h;
   const int np = (K1 + 1) / 2;
   const int ppb = slab_ppb(buf_elems, slab_plane_elems(K1, K2), K0);
-  const int x0 = (blockIdx.x - d.blk_y) * ppb, npl = min(ppb, K0 - x0);
+  const int x0 = (blockIdx.x - d.blk_slab) * ppb, npl = min(ppb, K0 - x0);
   const FastDiv fdK2 = fast_div(K2), fdK2h = fast_div(K2h), fdnp = fast_div(np), fdP = fast_div(K1 * K2h);
   Cplx<T>* W1 = reinterpret_cast<Cplx<T>*>(smem_raw);
   Cplx<T>* W2 = W1 + b.maxK1;
@@ -563,13 +567,13 @@ template <typename T>
 __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T>* __restrict__ spec,
                                                            T* __restrict__ mesh, int buf_elems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int s = find_sys<F_Y>(b, blockIdx.x);
+  const int s = find_sys<F_SLAB>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h;
   const int np = (K1 + 1) / 2;
   const int ppb = slab_ppb(buf_elems, slab_plane_elems(K1, K2), K0);
-  const int x0 = (blockIdx.x - d.blk_y) * ppb, npl = min(ppb, K0 - x0);
+  const int x0 = (blockIdx.x - d.blk_slab) * ppb, npl = min(ppb, K0 - x0);
   const FastDiv fdK2 = fast_div(K2), fdK2h = fast_div(K2h), fdnp = fast_div(np), fdP = fast_div(K1 * K2h);
   Cplx<T>* W1 = reinterpret_cast<Cplx<T>*>(smem_raw);
   Cplx<T>* W2 = W1 + b.maxK1;

@@ -21,6 +21,7 @@ static int recip_chunk_plan(int c0, int nsys, int N, const int* kmesh, double ka
 template <typename T>
 static size_t recip_ws_bytes(const RecipPlan<T>& p) {
   Carver c(nullptr, 0);
+  c.take<unsigned char>(sys_table_bytes());
   c.take<T>(p.mesh_elems);
   c.take<Cplx<T>>(p.spec_elems);
   c.take<double>((size_t)p.b.nsys * kAccStride);
@@ -52,10 +53,13 @@ static int pme_recip_impl(int nf, int N, const int* kmesh, const T* pos, const T
     int s = recip_chunk_plan<T>(c0, ns, N, kmesh, kappa, p);
     if (s) return s;
     Carver c(ws, bytes);
+    SysDesc* table = reinterpret_cast<SysDesc*>(c.take<unsigned char>(sys_table_bytes()));
     T* mesh = c.take<T>(p.mesh_elems);
     Cplx<T>* spec = c.take<Cplx<T>>(p.spec_elems);
     double* acc = c.take<double>((size_t)ns * kAccStride);
     if (!c.ok() || !ws) return fail(ADMP_ERR_WORKSPACE, "pme_recip workspace: need %zu bytes, got %zu", c.off, bytes);
+    s = bind_plan<T>(p, table, st);
+    if (s) return s;
     ADMP_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * ns * kAccStride, st));
     const size_t ao = (size_t)c0 * N;
     s = launch_recip<T>(p, pos + ao * 3, box + (size_t)c0 * 9, q + ao, mesh, spec, acc, ke, dq ? dq + ao : nullptr,

@@ -11,6 +11,7 @@ namespace admp {
 template <typename T>
 struct QEqWS {
   RecipPlan<T> plan;
+  SysDesc* table;
   T* mesh;
   Cplx<T>* spec;
   T* green;
@@ -39,6 +40,7 @@ static int qeq_carve(QEqWS<T>& w, void* ws, size_t bytes, int nf, int N, long lo
   if (s) return s;
   const size_t NT = (size_t)nf * N;
   Carver c(ws, bytes);
+  w.table = reinterpret_cast<SysDesc*>(c.take<unsigned char>(sys_table_bytes()));
   w.mesh = c.take<T>((flags & ADMP_QEQ_KSPACE) ? w.plan.mesh_elems : 0);
   w.spec = c.take<Cplx<T>>((flags & ADMP_QEQ_KSPACE) ? w.plan.spec_elems : 0);
   w.green = c.take<T>((flags & ADMP_QEQ_KSPACE) ? w.plan.spec_elems : 0);
@@ -130,6 +132,8 @@ static int qeq_solve_impl(int flags, int nf, int N, const int* kmesh, const T* p
   int s = qeq_carve<T>(c.w, ws, bytes, nf, N, Pn, kmesh, kappa, flags);
   if (s) return s;
   if (!ws || c.w.bytes > bytes) return fail(ADMP_ERR_WORKSPACE, "qeq workspace: need %zu bytes, got %zu", c.w.bytes, bytes);
+  s = bind_plan<T>(c.w.plan, c.w.table, st);
+  if (s) return s;
   c.P.flags = flags;
   c.P.axis = (flags >> 8) & 3;
   c.P.max_iter = max_iter;
@@ -221,14 +225,16 @@ static int qeq_solve_impl(int flags, int nf, int N, const int* kmesh, const T* p
 }
 
 template <typename T>
-static int qeq_hvp_impl(int flags, int N, const int* kmesh, const T* pos, const T* box, long long Pn,
+static int qeq_hvp_impl(int flags, int nf, int N, const int* kmesh, const T* pos, const T* box, long long Pn,
                         const long long* pairs, const T* ds, const T* bs, const T* hard, const T* eta, double kappa,
                         double ke, const T* p, T* out, void* ws, size_t bytes, cudaStream_t st) {
   QEqCtx<T> c;
-  int s = qeq_carve<T>(c.w, ws, bytes, 1, N, Pn, kmesh, kappa, flags);
+  int s = qeq_carve<T>(c.w, ws, bytes, nf, N, Pn, kmesh, kappa, flags);
   if (s) return s;
   if (!ws || c.w.bytes > bytes) return fail(ADMP_ERR_WORKSPACE, "qeq workspace: need %zu bytes, got %zu", c.w.bytes, bytes);
-  c.nf = 1;
+  s = bind_plan<T>(c.w.plan, c.w.table, st);
+  if (s) return s;
+  c.nf = nf;
   c.P.flags = flags;
   c.P.axis = (flags >> 8) & 3;
   c.P.max_iter = 0;
@@ -249,7 +255,7 @@ static int qeq_hvp_impl(int flags, int N, const int* kmesh, const T* pos, const 
                                                      nullptr);
   s = qeq_matvec<T>(c, p, c.w.Hp, nullptr);
   if (s) return s;
-  ADMP_CUDA_TRY(cudaMemcpyAsync(out, c.w.Hp, sizeof(T) * N, cudaMemcpyDeviceToDevice, st));
+  ADMP_CUDA_TRY(cudaMemcpyAsync(out, c.w.Hp, sizeof(T) * N * (size_t)nf, cudaMemcpyDeviceToDevice, st));
   DevError* err = scratch_error(st);
   return err ? check_error(err, st) : ADMP_OK;
 }
@@ -327,23 +333,38 @@ extern "C" int admp_qeq_solve(int dtype, int flags, int natoms, const int* kmesh
                                workspace, workspace_bytes, stream);
 }
 
-extern "C" int admp_qeq_hvp(int dtype, int flags, int natoms, const int* kmesh, const void* pos, const void* box,
-                            long long npairs, const long long* pairs, const void* ds, const void* buffer_scales,
-                            const void* hardness, const void* eta, double kappa, double ke, const void* p, void* out,
-                            void* workspace, size_t workspace_bytes, void* stream) {
+extern "C" int admp_qeq_hvp_frames(int dtype, int flags, int nframes, int natoms, const int* kmesh, const void* pos,
+                                   const void* box, long long npairs, const long long* pairs, const void* ds,
+                                   const void* buffer_scales, const void* hardness, const void* eta, double kappa,
+                                   double ke, const void* p, void* out, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+  if (nframes <= 0 || nframes > kMaxBatch)
+    return fail(ADMP_ERR_BAD_ARG, "admp_qeq_hvp: %d frames (1..%d)", nframes, kMaxBatch);
   if (natoms <= 0 || !pos || !box || !hardness || !p || !out) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_hvp: args");
   if ((flags & ADMP_QEQ_KSPACE) && (!kmesh || !(kappa > 0))) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_hvp: kspace needs kmesh and kappa");
   if ((flags & ADMP_QEQ_DAMPING) && !eta) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_hvp: damping needs eta");
+  if (npairs > 0 && (!pairs || !ds || !buffer_scales)) return fail(ADMP_ERR_BAD_ARG, "admp_qeq_hvp: pairs");
+  std::vector<int> K(3 * (size_t)nframes, 1);
+  if (flags & ADMP_QEQ_KSPACE)
+    for (size_t k = 0; k < K.size(); ++k) K[k] = kmesh[k];
   cudaStream_t st = (cudaStream_t)stream;
   if (dtype == ADMP_F64)
-    return qeq_hvp_impl<double>(flags, natoms, kmesh, (const double*)pos, (const double*)box, npairs, pairs,
-                                (const double*)ds, (const double*)buffer_scales, (const double*)hardness,
+    return qeq_hvp_impl<double>(flags, nframes, natoms, K.data(), (const double*)pos, (const double*)box, npairs,
+                                pairs, (const double*)ds, (const double*)buffer_scales, (const double*)hardness,
                                 (const double*)eta, kappa, ke, (const double*)p, (double*)out, workspace,
                                 workspace_bytes, st);
   if (dtype == ADMP_F32)
-    return qeq_hvp_impl<float>(flags, natoms, kmesh, (const float*)pos, (const float*)box, npairs, pairs,
+    return qeq_hvp_impl<float>(flags, nframes, natoms, K.data(), (const float*)pos, (const float*)box, npairs, pairs,
                                (const float*)ds, (const float*)buffer_scales, (const float*)hardness,
                                (const float*)eta, kappa, ke, (const float*)p, (float*)out, workspace, workspace_bytes,
                                st);
   return fail(ADMP_ERR_BAD_ARG, "bad dtype");
+}
+
+extern "C" int admp_qeq_hvp(int dtype, int flags, int natoms, const int* kmesh, const void* pos, const void* box,
+                            long long npairs, const long long* pairs, const void* ds, const void* buffer_scales,
+                            const void* hardness, const void* eta, double kappa, double ke, const void* p, void* out,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+  return admp_qeq_hvp_frames(dtype, flags, 1, natoms, kmesh, pos, box, npairs, pairs, ds, buffer_scales, hardness,
+                             eta, kappa, ke, p, out, workspace, workspace_bytes, stream);
 }

@@ -41,13 +41,20 @@ __global__ void srv_table_kernel(SrvLaunch L, const void* box_v, int dbl, const 
   }
 }
 
-__global__ void slot_export_kernel(Batch b, const CGScal* __restrict__ sc, int* __restrict__ slot_info) {
+// done flag, iterations, status and (optionally) the residual ||P grad||_2 / N
+// of the latest iterate of each listed QEq slot
+__global__ void slot_export_kernel(Batch b, const CGScal* __restrict__ sc, int* __restrict__ slot_info,
+                                   double* __restrict__ slot_resid) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= b.nsys) return;
   const int sl = b.s[s].box_idx;
   slot_info[4 * sl + 0] = sc[sl].done;
   slot_info[4 * sl + 1] = sc[sl].iter;
   if (sc[sl].status) slot_info[4 * sl + 2] = sc[sl].status;
+  if (slot_resid) {
+    const double rr = sc[sl].rr_new;  // the latest residual (init and every update leave it there)
+    slot_resid[sl] = sqrt(rr > 0.0 ? rr : 0.0) / (double)(b.s[s].natoms > 0 ? b.s[s].natoms : 1);
+  }
 }
 
 __global__ void slot_reset_kernel(Batch b, CGScal* __restrict__ sc, int nc) {
@@ -105,9 +112,12 @@ struct SrvCtx {
   size_t cells_need;
 };
 
+// per-system scratch of a call, after the system table at the head of sys_scratch
+static SrvSys* srv_sys(const admp_pools* P) { return (SrvSys*)((char*)P->sys_scratch + sys_table_bytes()); }
+
 template <typename T>
 static int srv_build(const admp_pools* P, const admp_sys* sys, int nsys, RecipPlan<T>& plan, SrvCtx& c,
-                     bool need_mesh) {
+                     bool need_mesh, cudaStream_t stream) {
   if (nsys <= 0 || nsys > kMaxBatch) return fail(ADMP_ERR_BAD_ARG, "serve: %d systems per call (1..%d)", nsys, kMaxBatch);
   SysSpec spec[kMaxBatch];
   size_t coff = 0;
@@ -134,14 +144,18 @@ static int srv_build(const admp_pools* P, const admp_sys* sys, int nsys, RecipPl
   c.cells_need = coff;
   int st = build_recip_plan<T>(spec, nsys, plan);
   if (st) return st;
-  for (int s = 0; s < nsys; ++s) plan.b.s[s].flags = sys[s].kind;
-  c.L.b = plan.b;
+  for (int s = 0; s < nsys; ++s) plan.hs[s].flags = sys[s].kind;
   if (need_mesh) {
     if ((long long)plan.mesh_elems > P->mesh_cap || (long long)plan.spec_elems > P->spec_cap || nsys > P->acc_cap)
       return fail(ADMP_ERR_WORKSPACE, "serve: mesh pool too small (need %zu real, %zu complex)", plan.mesh_elems,
                   plan.spec_elems);
   }
-  if ((size_t)P->sys_scratch_bytes < sizeof(SrvSys) * nsys) return fail(ADMP_ERR_WORKSPACE, "serve: sys scratch too small");
+  if ((size_t)P->sys_scratch_bytes < sys_table_bytes() + sizeof(SrvSys) * nsys)
+    return fail(ADMP_ERR_WORKSPACE, "serve: sys scratch too small");
+  // the call's system table goes to the head of the sys scratch; its launches follow on the same stream
+  st = bind_plan<T>(plan, (SysDesc*)P->sys_scratch, stream);
+  if (st) return st;
+  c.L.b = plan.b;
   return ADMP_OK;
 }
 
@@ -149,10 +163,10 @@ template <typename T>
 static int serve_neighbors_impl(const admp_pools* P, const admp_sys* sys, int nsys, cudaStream_t st) {
   RecipPlan<T> plan;
   SrvCtx c;
-  int s = srv_build<T>(P, sys, nsys, plan, c, false);
+  int s = srv_build<T>(P, sys, nsys, plan, c, false, st);
   if (s) return s;
   if ((long long)c.cells_need > P->cells_cap) return fail(ADMP_ERR_WORKSPACE, "serve: cell pool too small (%zu)", c.cells_need);
-  SrvSys* ss = (SrvSys*)P->sys_scratch;
+  SrvSys* ss = srv_sys(P);
   const Batch& b = plan.b;
   typedef typename Vec4<T>::type V4;
   const int hn = prof_begin(st);
@@ -164,6 +178,10 @@ static int serve_neighbors_impl(const admp_pools* P, const admp_sys* sys, int ns
                                                 P->pos64 ? (double4*)P->frac64 : nullptr, P->cell_of, P->cells,
                                                 P->pcnt, P->pstart);
   sn_scan_cells_kernel<<<nsys, 1024, 0, st>>>(ss, P->cells);
+  if (P->celltab) {
+    sn_celltab_kernel<<<nsys, 256, 0, st>>>(b, ss, P->cells, P->celltab, P->celltab_stride);
+    count_launches(1);
+  }
   sn_scatter_kernel<<<b.nblk_atom, 256, 0, st>>>(b, ss, P->cell_of, P->cells, P->sorted);
   sn_pairs_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, f64, P->cell_of, P->cells, P->sorted,
                                                   P->pcnt, P->pstart, P->col);
@@ -178,9 +196,9 @@ template <typename T>
 static int serve_ef_impl(const admp_pools* P, const admp_sys* sys, int nsys, double ke, cudaStream_t st) {
   RecipPlan<T> plan;
   SrvCtx c;
-  int s = srv_build<T>(P, sys, nsys, plan, c, true);
+  int s = srv_build<T>(P, sys, nsys, plan, c, true, st);
   if (s) return s;
-  SrvSys* ss = (SrvSys*)P->sys_scratch;
+  SrvSys* ss = srv_sys(P);
   const Batch& b = plan.b;
   typedef typename Vec4<T>::type V4;
   srv_table_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(c.L, P->box, sizeof(T) == 8, P->slot_info, ss, 0);
@@ -194,7 +212,7 @@ static int serve_ef_impl(const admp_pools* P, const admp_sys* sys, int nsys, dou
   count_launches(6);
   ADMP_CUDA_TRY(cudaMemsetAsync(P->acc, 0, sizeof(double) * kAccStride * nsys, st));
   s = launch_recip<T>(plan, (const T*)P->pos, (const T*)P->box, (const T*)P->q, (T*)P->mesh, (Cplx<T>*)P->spec,
-                      P->acc, ke, nullptr, (T*)P->force, st, P->sorted);
+                      P->acc, ke, nullptr, (T*)P->force, st, P->sorted, P->celltab, P->celltab_stride);
   if (s) return s;
   recip_finalize_kernel<T><<<(nsys + 127) / 128, 128, 0, st>>>(b, (const T*)P->box, P->acc, P->energy, nullptr);
   sys_terms_kernel<T><<<nsys, 512, 0, st>>>(b, ss, (const T*)P->q, (const T*)P->chi, (const T*)P->hardness,
@@ -293,7 +311,8 @@ static int srv_matvec(const admp_pools* P, const RecipPlan<T>& plan, QEqParams p
                       double* hv_out, double ke, cudaStream_t st) {
   const Batch& b = plan.b;
   int s = launch_recip_potential<T>(plan, (const T*)P->pos, (const T*)P->box, v, (T*)P->mesh, (Cplx<T>*)P->spec,
-                                    P->acc, ke, Hv, st, P->sorted, (const T*)P->green);
+                                    P->acc, ke, Hv, st, P->sorted, (const T*)P->green, P->celltab,
+                                    P->celltab_stride);
   if (s) return s;
   int h = prof_begin(st);
   csr_spmv_finish_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, P->pstart, P->pcnt, P->col, (const T*)P->coef, v,
@@ -319,9 +338,9 @@ static int serve_qeq_init_impl(const admp_pools* P, const admp_sys* sys, int nsy
                                double ke, cudaStream_t st) {
   RecipPlan<T> plan;
   SrvCtx c;
-  int s = srv_build<T>(P, sys, nsys, plan, c, true);
+  int s = srv_build<T>(P, sys, nsys, plan, c, true, st);
   if (s) return s;
-  SrvSys* ss = (SrvSys*)P->sys_scratch;
+  SrvSys* ss = srv_sys(P);
   const Batch& b = plan.b;
   typedef typename Vec4<T>::type V4;
   CGScal* sc = (CGScal*)P->cg_state;
@@ -358,7 +377,7 @@ static int serve_qeq_init_impl(const admp_pools* P, const admp_sys* sys, int nsy
   qeq_resid_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, P->cg_hx, P->cg_chi, (const T*)nullptr, 0, P->cg_z, P->cg_r,
                                                    (T*)P->cg_p, sc, 1);
   qeq_init_done_kernel<<<(nsys + 31) / 32, 32, 0, st>>>(b, prm, sc);
-  slot_export_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc, P->slot_info);
+  slot_export_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc, P->slot_info, P->slot_resid);
   count_launches(18);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
@@ -369,7 +388,7 @@ static int serve_qeq_iterate_impl(const admp_pools* P, const admp_sys* sys, int 
                                   int max_iter, double ke, cudaStream_t st) {
   RecipPlan<T> plan;
   SrvCtx c;
-  int s = srv_build<T>(P, sys, nsys, plan, c, true);
+  int s = srv_build<T>(P, sys, nsys, plan, c, true, st);
   if (s) return s;
   CGScal* sc = (CGScal*)P->cg_state;
   plan.b.done = &sc[0].done;
@@ -387,7 +406,7 @@ static int serve_qeq_iterate_impl(const admp_pools* P, const admp_sys* sys, int 
     qeq_direction_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, P->cg_r, (T*)P->cg_p, P->cg_z, sc);
     prof_end(hv, PK_CG_VECTOR, -1.0, st);
   }
-  slot_export_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc, P->slot_info);
+  slot_export_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(b, sc, P->slot_info, P->slot_resid);
   count_launches(1);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
@@ -397,7 +416,7 @@ template <typename T>
 static int serve_qeq_finish_impl(const admp_pools* P, const admp_sys* sys, int nsys, cudaStream_t st) {
   RecipPlan<T> plan;
   SrvCtx c;
-  int s = srv_build<T>(P, sys, nsys, plan, c, false);
+  int s = srv_build<T>(P, sys, nsys, plan, c, false, st);
   if (s) return s;
   const Batch& b = plan.b;
   cast_atoms_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, nullptr, nullptr, 0, (T*)P->q, P->cg_x);
@@ -411,7 +430,9 @@ static int serve_qeq_finish_impl(const admp_pools* P, const admp_sys* sys, int n
 using namespace admp;
 
 extern "C" size_t admp_serve_slot_state_bytes(void) { return sizeof(CGScal); }
-extern "C" size_t admp_serve_sys_scratch_bytes(int nsys) { return sizeof(SrvSys) * (size_t)(nsys > 0 ? nsys : 1); }
+extern "C" size_t admp_serve_sys_scratch_bytes(int nsys) {
+  return sys_table_bytes() + sizeof(SrvSys) * (size_t)(nsys > 0 ? nsys : 1);
+}
 extern "C" size_t admp_serve_cells_needed(const admp_sys* sys, int nsys) {
   size_t c = 0;
   for (int s = 0; s < nsys; ++s) c += 3 * (size_t)(2 * sys[s].natoms + 128 + 1);

@@ -67,6 +67,8 @@ def parse():
                     help="open-loop Poisson arrival rate (requests/s) for p50/p99")
     ap.add_argument("--cpu-reps", type=int, default=None,
                     help="repetitions of the CPU sample (default 3 for --impl reference, 1 beside the GPU arm)")
+    ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE,
+                    help="requests in the size-stratified CPU sample")
     ap.add_argument("--plain-sample", type=int, default=100)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
@@ -139,7 +141,7 @@ def cpu_sample(stream, k: int = CPU_SAMPLE):
     return [srt[min(n - 1, int((j + 0.5) * n / k))] for j in range(min(k, n))]
 
 
-def cpu_baseline(stream, reps: int = 1):
+def cpu_baseline(stream, reps: int = 1, k: int = CPU_SAMPLE):
     """CPU oracle throughput, measured: the size-stratified sample of the
     stream runs on every host core at once (spawn pool, one request per
     task, largest first), timed by the wall clock; value = sample requests /
@@ -149,7 +151,7 @@ def cpu_baseline(stream, reps: int = 1):
     cores, description, details dict)."""
     import multiprocessing as mp
     cores = os.cpu_count() or 1
-    picks = cpu_sample(stream)
+    picks = cpu_sample(stream, k)
     order = sorted(range(len(picks)), key=lambda j: -(picks[j].natoms * (8 if picks[j].kind == "qeq" else 1)))
     tasks = [(picks[j].kind, picks[j].pos, picks[j].box, picks[j].charges, picks[j].chi, picks[j].hardness,
               picks[j].eta) for j in order]
@@ -489,7 +491,7 @@ def main():
         if rank != 0:
             return
         stream = synthetic.serving_stream(args.nreq, SEED, RATE)
-        v, cores, sample, det = cpu_baseline(stream, args.cpu_reps or 3)
+        v, cores, sample, det = cpu_baseline(stream, args.cpu_reps or 3, args.cpu_sample)
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -660,9 +662,9 @@ def main():
     cpu = None
     same = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sample_reqs = cpu_sample(stream)
+        sample_reqs = cpu_sample(stream, args.cpu_sample)
         same = same_sample_gpu(eng, sample_reqs)
-        v, cores, sample, det = cpu_baseline(stream, args.cpu_reps or 1)
+        v, cores, sample, det = cpu_baseline(stream, args.cpu_reps or 1, args.cpu_sample)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
                "extrapolated_stream_value": det["extrapolated_stream_value"]}
         same["cpu_value"] = v

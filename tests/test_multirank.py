@@ -36,7 +36,7 @@ def test_replicas_max_over_ranks_and_own_streams(tmp_path):
 
 def test_reference_arm_two_ranks_reports_once():
     p = _torchrun(["bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0",
-                   "--nreq", "24", "--cpu-seconds", "5"], timeout=600)
+                   "--nreq", "24", "--cpu-sample", "3", "--cpu-reps", "1"], timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
     lines = [json.loads(ln) for ln in p.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1

@@ -1,16 +1,15 @@
-// Brick-privatised spread and gather for atoms binned in neighbour cells
-// (the serving path, whose neighbour build sorts every system's atoms by
-// cell).  Same arithmetic as spread_kernel / gather_kernel (recip.py:146-252
-// and the autograd of pme.py:351-446); only the memory traffic differs.
+// Brick-privatised spread for atoms binned in neighbour cells (the serving
+// path, whose neighbour build sorts every system's atoms by cell).  Same
+// arithmetic as spread_kernel (recip.py:146-252); only the memory traffic
+// differs.
 //
 // A brick is a run of G cells along z inside one (x, y) cell column.  The
 // stencils of its atoms cover a box of mesh points ("tile"): the brick's
 // mesh extent plus the 6-point stencil reach, or the whole period along an
-// axis where that box would wrap onto itself.  spread accumulates the tile
-// in shared memory and adds it to the mesh row by row (coalesced global
-// reductions, one per tile point instead of 216 scattered ones per atom);
-// gather loads the tile once and every atom reads its 216 points from shared
-// memory.  An atom whose stencil falls outside its brick's tile (possible
+// axis where that box would wrap onto itself.  The kernel accumulates the
+// tile in shared memory and adds it to the mesh row by row (coalesced global
+// reductions, one per tile point instead of 216 scattered ones per atom).
+// An atom whose stencil falls outside its brick's tile (possible
 // only within rounding of a cell face, since the binning and the stencil
 // compute the fractional coordinate from different copies of the position)
 // takes the direct global path, so the result never depends on the binning.
@@ -25,13 +24,6 @@
 namespace admp {
 
 constexpr int kCellHdr = 4;
-
-// tile capacity (elements of T) per kernel: shared memory is the tile plus
-// 8 warps' stencils, sized for two blocks per SM
-template <typename T, bool FORCES>
-__host__ __device__ constexpr int brick_cap() {
-  return sizeof(T) == 4 ? (FORCES ? 16000 : 18000) : (FORCES ? 8000 : 9000);
-}
 
 struct TileAxis {
   int o, w, K;
@@ -133,38 +125,37 @@ __device__ __forceinline__ Brick brick_at(const int* ct, const SysDesc& d, const
   return k;
 }
 
-// Per-warp stencils of 32 atoms: 18 weights (and derivatives), the wrapped
-// stencil bases per axis, the charge and the atom index.
-template <typename T, bool DERIV>
+// Per-warp stencils of 32 atoms, laid out for the accumulation loop: the 18
+// weights, the charge, the tile offsets of the atom's 6 x planes (-1 when
+// the stencil does not fit the tile), of its 6 y rows and 6 z points, and
+// the wrapped mesh bases for the atoms that take the direct path.
+template <typename T>
 struct BrickStencil {
-  T* w;      // [32][18]
-  T* dw;     // [32][18]
-  T* q;      // [32]
-  int* b3;   // [32][3]
-  int* atom; // [32]
+  T* w;          // [32][18]
+  T* q;          // [32]
+  int* ox;       // [32][6]  tile offset of plane x (times wy wz)
+  short* oy;     // [32][6]  tile offset of row y (times wz)
+  short* oz;     // [32][6]  tile offset of point z
+  int* b3;       // [32][3]  wrapped mesh bases
   __host__ __device__ static constexpr size_t bytes() {
-    return 32 * 18 * sizeof(T) * (DERIV ? 2 : 1) + 32 * sizeof(T) + 32 * 3 * sizeof(int) + 32 * sizeof(int) + 16;
+    return 32 * 18 * sizeof(T) + 32 * sizeof(T) + 32 * 6 * sizeof(int) + 2 * 32 * 6 * sizeof(short) +
+           32 * 3 * sizeof(int) + 16;
   }
   __device__ void carve(unsigned char* base) {
     w = reinterpret_cast<T*>(base);
-    T* e = w + 32 * 18;
-    if (DERIV) {
-      dw = e;
-      e += 32 * 18;
-    } else {
-      dw = nullptr;
-    }
-    q = e;
-    b3 = reinterpret_cast<int*>(q + 32);
-    atom = b3 + 32 * 3;
+    q = w + 32 * 18;
+    ox = reinterpret_cast<int*>(q + 32);
+    b3 = ox + 32 * 6;
+    oy = reinterpret_cast<short*>(b3 + 32 * 3);
+    oz = oy + 32 * 6;
   }
 };
 
-template <typename T, bool DERIV>
-__device__ __forceinline__ void brick_build_stencil(BrickStencil<T, DERIV>& ws, const SysDesc& d, const Geom& g,
-                                                    const T* __restrict__ pos, const T* __restrict__ q,
-                                                    const int* __restrict__ order, int a_first, int a_end,
-                                                    int lane) {
+template <typename T>
+__device__ __forceinline__ void brick_build_stencil(BrickStencil<T>& ws, const SysDesc& d, const Geom& g,
+                                                    const Brick& k, const T* __restrict__ pos,
+                                                    const T* __restrict__ q, const int* __restrict__ order,
+                                                    int a_first, int a_end, int lane) {
   const int a = a_first + lane;
   if (a < a_end) {
     const int ga = order[d.atom_off + a];
@@ -173,326 +164,131 @@ __device__ __forceinline__ void brick_build_stencil(BrickStencil<T, DERIV>& ws, 
     make_stencil<T>(r, g, d.K0, d.K1, d.K2, st);
     T* w = ws.w + lane * 18;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      w[k] = st.w[0][k];
-      w[6 + k] = st.w[1][k];
-      w[12 + k] = st.w[2][k];
+    for (int j = 0; j < 6; ++j) {
+      w[j] = st.w[0][j];
+      w[6 + j] = st.w[1][j];
+      w[12 + j] = st.w[2][j];
     }
-    if (DERIV) {
-      T* dw = ws.dw + lane * 18;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        dw[k] = st.dw[0][k];
-        dw[6 + k] = st.dw[1][k];
-        dw[12 + k] = st.dw[2][k];
-      }
-    }
+    ws.q[lane] = q[ga];
     ws.b3[lane * 3] = st.ix[0];
     ws.b3[lane * 3 + 1] = st.iy[0];
     ws.b3[lane * 3 + 2] = st.iz[0];
-    ws.q[lane] = q ? q[ga] : T(0);
-    ws.atom[lane] = ga;
+    const int tx = tile_start(k.ax, st.ix[0]), ty = tile_start(k.ay, st.iy[0]), tz = tile_start(k.az, st.iz[0]);
+    const bool fit = tx >= 0 && ty >= 0 && tz >= 0;
+    const int wyz = k.ay.w * k.az.w;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      ws.ox[lane * 6 + j] = fit ? tile_at(k.ax, tx, j) * wyz : -1;
+      ws.oy[lane * 6 + j] = (short)(fit ? tile_at(k.ay, ty, j) * k.az.w : 0);
+      ws.oz[lane * 6 + j] = (short)(fit ? tile_at(k.az, tz, j) : 0);
+    }
   }
   __syncwarp();
 }
 
-template <typename T, bool FORCES>
+// tile capacity (elements of T) of the spread, and its dynamic shared memory:
+// the tile plus 8 warps' stencils, sized for three blocks per SM
+template <typename T>
+__host__ __device__ constexpr int brick_cap() {
+  return sizeof(T) == 4 ? 10000 : 5000;
+}
+
+template <typename T>
 inline size_t brick_smem() {
-  return (size_t)brick_cap<T, FORCES>() * sizeof(T) + 8 * BrickStencil<T, FORCES>::bytes() + 64;
+  return (size_t)brick_cap<T>() * sizeof(T) + 8 * BrickStencil<T>::bytes() + 64;
+}
+
+// one stencil column (lanes y0, z0) of atom j: into the tile, or into the mesh
+template <typename T>
+__device__ __forceinline__ void brick_column(const BrickStencil<T>& ws, int j, int y0, int z0, T* tile, T* M,
+                                             const SysDesc& d, int K1K2) {
+  const T qa = ws.q[j];
+  const T* w = ws.w + j * 18;
+  const T v = qa * w[6 + y0] * w[12 + z0];
+  const int* ox = ws.ox + j * 6;
+  if (ox[0] >= 0) {
+    T* t = tile + ws.oy[j * 6 + y0] + ws.oz[j * 6 + z0];
+#pragma unroll
+    for (int dx = 0; dx < 6; ++dx) atomicAdd(t + ox[dx], w[dx] * v);
+  } else {
+    const int* bb = ws.b3 + 3 * j;
+    T* m = M + wrap_up(bb[1] + y0, d.K1) * d.K2 + wrap_up(bb[2] + z0, d.K2);
+#pragma unroll
+    for (int dx = 0; dx < 6; ++dx) atomicAdd(m + wrap_up(bb[0] + dx, d.K0) * K1K2, w[dx] * v);
+  }
 }
 
 // ---------------------------------------------------------------------------
 // spread into the zeroed mesh
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256, 2) spread_brick_kernel(Batch b, const T* __restrict__ pos,
-                                                           const T* __restrict__ box, const T* __restrict__ q,
-                                                           T* __restrict__ mesh, const int* __restrict__ order,
-                                                           const int* __restrict__ cells, int cell_stride) {
+__global__ void __launch_bounds__(256, 3) spread_brick_kernel(Batch b, const T* __restrict__ pos,
+                                                              const T* __restrict__ box, const T* __restrict__ q,
+                                                              T* __restrict__ mesh, const int* __restrict__ order,
+                                                              const int* __restrict__ cells, int cell_stride) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ Geom g;
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
   const SysDesc& d = b.s[s];
-  constexpr int cap = brick_cap<T, false>();
+  constexpr int cap = brick_cap<T>();
   T* tile = reinterpret_cast<T*>(dsm);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  BrickStencil<T, false> ws;
-  ws.carve(dsm + (size_t)cap * sizeof(T) + warp * BrickStencil<T, false>::bytes());
+  BrickStencil<T> ws;
+  ws.carve(dsm + (size_t)cap * sizeof(T) + warp * BrickStencil<T>::bytes());
   load_geom(box, d.box_idx, &g);
   __syncthreads();
   const int* ct = cells + (size_t)d.box_idx * cell_stride;
-  const BrickPlan p = brick_plan(ct, d, cap);
+  BrickPlan p = brick_plan(ct, d, cap);
   const int jb = blockIdx.x - d.blk_atom;
   const int nblk = (d.natoms + b.apb - 1) / b.apb;
   T* M = mesh + d.mesh_off;
   const int K1K2 = d.K1 * d.K2;
   // lanes over the first 32 (y, z) stencil columns; the last four columns of eight atoms in one pass
   const int y0 = lane / 6, z0 = lane % 6, jt = lane >> 2, zt = 2 + (lane & 3);
-  if (p.G == 0) {  // no brick fits: this block's chunk of the sorted atoms with global reductions
-    const int a_begin = jb * b.apb, a_end = min(a_begin + b.apb, d.natoms);
-    for (int a0 = a_begin + warp * 32; a0 < a_end; a0 += nw * 32) {
-      brick_build_stencil<T, false>(ws, d, g, pos, q, order, a0, a_end, lane);
-      const int na = min(32, a_end - a0);
-      for (int j = 0; j < na; ++j) {
-        const T qa = ws.q[j];
-        const T* w = ws.w + j * 18;
-        for (int c = lane; c < 36; c += 32) {
-          const int yy = c / 6, zz = c - 6 * (c / 6);
-          const T wyz = qa * w[6 + yy] * w[12 + zz];
-          const int oyz = wrap_up(ws.b3[3 * j + 1] + yy, d.K1) * d.K2 + wrap_up(ws.b3[3 * j + 2] + zz, d.K2);
-#pragma unroll
-          for (int dx = 0; dx < 6; ++dx) atomicAdd(M + wrap_up(ws.b3[3 * j] + dx, d.K0) * K1K2 + oyz, w[dx] * wyz);
-        }
-      }
-      __syncwarp();
-    }
-    return;
-  }
-  for (int br = jb; br < p.nbricks; br += nblk) {
-    const Brick k = brick_at(ct, d, p, br);
-    const int n = k.ax.w * k.ay.w * k.az.w;
-    const int wyz = k.ay.w * k.az.w;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) tile[i] = T(0);
-    __syncthreads();
-    for (int a0 = k.a0 + warp * 32; a0 < k.a1; a0 += nw * 32) {
-      brick_build_stencil<T, false>(ws, d, g, pos, q, order, a0, k.a1, lane);
-      const int na = min(32, k.a1 - a0);
-      for (int j0 = 0; j0 < na; j0 += 8) {
-        const int j1 = min(j0 + 8, na);
-        for (int j = j0; j < j1; ++j) {
-          const T qa = ws.q[j];
-          if (qa == T(0)) continue;
-          const T* w = ws.w + j * 18;
-          const int* bb = ws.b3 + 3 * j;
-          const int tx = tile_start(k.ax, bb[0]), ty = tile_start(k.ay, bb[1]), tz = tile_start(k.az, bb[2]);
-          const T v = qa * w[6 + y0] * w[12 + z0];
-          if (tx >= 0 && ty >= 0 && tz >= 0) {
-            const int oyz = tile_at(k.ay, ty, y0) * k.az.w + tile_at(k.az, tz, z0);
-#pragma unroll
-            for (int dx = 0; dx < 6; ++dx) atomicAdd(tile + tile_at(k.ax, tx, dx) * wyz + oyz, w[dx] * v);
-          } else {
-            const int oyz = wrap_up(bb[1] + y0, d.K1) * d.K2 + wrap_up(bb[2] + z0, d.K2);
-#pragma unroll
-            for (int dx = 0; dx < 6; ++dx) atomicAdd(M + wrap_up(bb[0] + dx, d.K0) * K1K2 + oyz, w[dx] * v);
-          }
-        }
-        const int j = j0 + jt;
-        if (j < j1) {
-          const T qa = ws.q[j];
-          if (qa != T(0)) {
-            const T* w = ws.w + j * 18;
-            const int* bb = ws.b3 + 3 * j;
-            const int tx = tile_start(k.ax, bb[0]), ty = tile_start(k.ay, bb[1]), tz = tile_start(k.az, bb[2]);
-            const T v = qa * w[6 + 5] * w[12 + zt];
-            if (tx >= 0 && ty >= 0 && tz >= 0) {
-              const int oyz = tile_at(k.ay, ty, 5) * k.az.w + tile_at(k.az, tz, zt);
-#pragma unroll
-              for (int dx = 0; dx < 6; ++dx) atomicAdd(tile + tile_at(k.ax, tx, dx) * wyz + oyz, w[dx] * v);
-            } else {
-              const int oyz = wrap_up(bb[1] + 5, d.K1) * d.K2 + wrap_up(bb[2] + zt, d.K2);
-#pragma unroll
-              for (int dx = 0; dx < 6; ++dx) atomicAdd(M + wrap_up(bb[0] + dx, d.K0) * K1K2 + oyz, w[dx] * v);
-            }
-          }
-        }
-      }
-      __syncwarp();
-    }
-    __syncthreads();
-    // add the tile to the mesh, one warp per tile row (consecutive z)
-    for (int r = warp; r < k.ax.w * k.ay.w; r += nw) {
-      const int tx = r / k.ay.w, ty = r - tx * k.ay.w;
-      T* row = M + (size_t)tile_mesh(k.ax, tx) * K1K2 + (size_t)tile_mesh(k.ay, ty) * d.K2;
-      const T* src = tile + (size_t)r * k.az.w;
-      for (int tz = lane; tz < k.az.w; tz += 32) {
-        const T v = src[tz];
-        if (v != T(0)) atomicAdd(row + tile_mesh(k.az, tz), v);
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// ---------------------------------------------------------------------------
-// gather: pot_i = sum phi theta; dE/du_d = q sum phi dtheta/du_d
-// ---------------------------------------------------------------------------
-template <typename T, bool FORCES>
-__global__ void __launch_bounds__(256, 2) gather_brick_kernel(Batch b, const T* __restrict__ pos,
-                                                           const T* __restrict__ box, const T* __restrict__ q,
-                                                           const T* __restrict__ phi, T* __restrict__ dE_dq,
-                                                           T* __restrict__ dE_dpos, double* __restrict__ acc,
-                                                           T pot_scale, const int* __restrict__ order,
-                                                           const int* __restrict__ cells, int cell_stride) {
-  extern __shared__ __align__(16) unsigned char dsm[];
-  __shared__ Geom g;
-  __shared__ double red[9 * 32];
-  const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
-  constexpr int cap = brick_cap<T, FORCES>();
-  T* tile = reinterpret_cast<T*>(dsm);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  BrickStencil<T, FORCES> ws;
-  ws.carve(dsm + (size_t)cap * sizeof(T) + warp * BrickStencil<T, FORCES>::bytes());
-  load_geom(box, d.box_idx, &g);
-  __syncthreads();
-  const int* ct = cells + (size_t)d.box_idx * cell_stride;
-  const BrickPlan p = brick_plan(ct, d, cap);
-  const int jb = blockIdx.x - d.blk_atom;
-  const int nblk = (d.natoms + b.apb - 1) / b.apb;
-  const T* M = phi + d.mesh_off;
-  const int K1K2 = d.K1 * d.K2;
-  const int K[3] = {d.K0, d.K1, d.K2};
-  const int y0 = lane / 6, z0 = lane % 6, jt = lane >> 2, zt = 2 + (lane & 3);
-  double wf[9];
-#pragma unroll
-  for (int e = 0; e < 9; ++e) wf[e] = 0.0;
-  // without bricks (G = 0) the block makes one pass over its chunk of the sorted atoms, reading the mesh
+  // without bricks (G = 0) the block makes one pass over its chunk of the sorted atoms with every
+  // stencil taking the direct path (an empty tile: nothing fits)
   const bool direct = p.G == 0;
-  const int first = direct ? 0 : jb, last = direct ? 1 : p.nbricks, step = direct ? 1 : nblk;
-  for (int br = first; br < last; br += step) {
+  const int br0 = direct ? 0 : jb, br1 = direct ? 1 : p.nbricks, step = direct ? 1 : nblk;
+  for (int br = br0; br < br1; br += step) {
     Brick k;
     if (direct) {
       k.a0 = jb * b.apb;
       k.a1 = min(k.a0 + b.apb, d.natoms);
+      k.ax = {0, 0, d.K0, false};  // width 0: tile_start never fits
+      k.ay = k.ax;
+      k.az = k.ax;
     } else {
       k = brick_at(ct, d, p, br);
-      // load the tile, one warp per row of consecutive z
-      for (int r = warp; r < k.ax.w * k.ay.w; r += nw) {
-        const int tx = r / k.ay.w, ty = r - tx * k.ay.w;
-        const T* row = M + (size_t)tile_mesh(k.ax, tx) * K1K2 + (size_t)tile_mesh(k.ay, ty) * d.K2;
-        T* dst = tile + (size_t)r * k.az.w;
-        for (int tz = lane; tz < k.az.w; tz += 32) dst[tz] = row[tile_mesh(k.az, tz)];
-      }
-      __syncthreads();
+      const int n = k.ax.w * k.ay.w * k.az.w;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) tile[i] = T(0);
     }
+    __syncthreads();
     for (int a0 = k.a0 + warp * 32; a0 < k.a1; a0 += nw * 32) {
-      brick_build_stencil<T, FORCES>(ws, d, g, pos, q, order, a0, k.a1, lane);
+      brick_build_stencil<T>(ws, d, g, k, pos, q, order, a0, k.a1, lane);
       const int na = min(32, k.a1 - a0);
-      T my_pot = 0, my_g0 = 0, my_g1 = 0, my_g2 = 0;
       for (int j0 = 0; j0 < na; j0 += 8) {
         const int j1 = min(j0 + 8, na);
-        for (int j = j0; j < j1; ++j) {
-          const T* w = ws.w + j * 18;
-          const int* bb = ws.b3 + 3 * j;
-          T f[6];
-          const int tx = direct ? -1 : tile_start(k.ax, bb[0]);
-          const int ty = direct ? -1 : tile_start(k.ay, bb[1]);
-          const int tz = direct ? -1 : tile_start(k.az, bb[2]);
-          if (tx >= 0 && ty >= 0 && tz >= 0) {
-            const int wyz = k.ay.w * k.az.w;
-            const int oyz = tile_at(k.ay, ty, y0) * k.az.w + tile_at(k.az, tz, z0);
-#pragma unroll
-            for (int dx = 0; dx < 6; ++dx) f[dx] = tile[tile_at(k.ax, tx, dx) * wyz + oyz];
-          } else {
-            const int oyz = wrap_up(bb[1] + y0, d.K1) * d.K2 + wrap_up(bb[2] + z0, d.K2);
-#pragma unroll
-            for (int dx = 0; dx < 6; ++dx) f[dx] = M[wrap_up(bb[0] + dx, d.K0) * K1K2 + oyz];
-          }
-          const T wy = w[6 + y0], wz = w[12 + z0];
-          T sw = 0, sdw = 0;
-#pragma unroll
-          for (int dx = 0; dx < 6; ++dx) {
-            sw += f[dx] * w[dx];
-            if (FORCES) sdw += f[dx] * ws.dw[j * 18 + dx];
-          }
-          T pot = warp_sum(sw * wy * wz), g0 = 0, g1 = 0, g2 = 0;
-          if (FORCES) {
-            g0 = warp_sum(sdw * wy * wz);
-            g1 = warp_sum(sw * ws.dw[j * 18 + 6 + y0] * wz);
-            g2 = warp_sum(sw * wy * ws.dw[j * 18 + 12 + z0]);
-          }
-          if (lane == j) {
-            my_pot = pot;
-            my_g0 = g0;
-            my_g1 = g1;
-            my_g2 = g2;
-          }
-        }
-        // the last four columns of atoms j0 .. j1-1, reduced over each atom's four lanes
-        T pot = 0, g0 = 0, g1 = 0, g2 = 0;
-        const int j = j0 + jt;
-        if (j < j1) {
-          const T* w = ws.w + j * 18;
-          const int* bb = ws.b3 + 3 * j;
-          T f[6];
-          const int tx = direct ? -1 : tile_start(k.ax, bb[0]);
-          const int ty = direct ? -1 : tile_start(k.ay, bb[1]);
-          const int tz = direct ? -1 : tile_start(k.az, bb[2]);
-          if (tx >= 0 && ty >= 0 && tz >= 0) {
-            const int wyz = k.ay.w * k.az.w;
-            const int oyz = tile_at(k.ay, ty, 5) * k.az.w + tile_at(k.az, tz, zt);
-#pragma unroll
-            for (int dx = 0; dx < 6; ++dx) f[dx] = tile[tile_at(k.ax, tx, dx) * wyz + oyz];
-          } else {
-            const int oyz = wrap_up(bb[1] + 5, d.K1) * d.K2 + wrap_up(bb[2] + zt, d.K2);
-#pragma unroll
-            for (int dx = 0; dx < 6; ++dx) f[dx] = M[wrap_up(bb[0] + dx, d.K0) * K1K2 + oyz];
-          }
-          const T wy = w[6 + 5], wz = w[12 + zt];
-          T sw = 0, sdw = 0;
-#pragma unroll
-          for (int dx = 0; dx < 6; ++dx) {
-            sw += f[dx] * w[dx];
-            if (FORCES) sdw += f[dx] * ws.dw[j * 18 + dx];
-          }
-          pot = sw * wy * wz;
-          if (FORCES) {
-            g0 = sdw * wy * wz;
-            g1 = sw * ws.dw[j * 18 + 6 + 5] * wz;
-            g2 = sw * wy * ws.dw[j * 18 + 12 + zt];
-          }
-        }
-#pragma unroll
-        for (int o = 1; o < 4; o <<= 1) {
-          pot += __shfl_xor_sync(0xffffffffu, pot, o);
-          if (FORCES) {
-            g0 += __shfl_xor_sync(0xffffffffu, g0, o);
-            g1 += __shfl_xor_sync(0xffffffffu, g1, o);
-            g2 += __shfl_xor_sync(0xffffffffu, g2, o);
-          }
-        }
-        const int src = 4 * ((lane - j0) & 7);
-        pot = __shfl_sync(0xffffffffu, pot, src);
-        if (FORCES) {
-          g0 = __shfl_sync(0xffffffffu, g0, src);
-          g1 = __shfl_sync(0xffffffffu, g1, src);
-          g2 = __shfl_sync(0xffffffffu, g2, src);
-        }
-        if (lane >= j0 && lane < j1) {
-          my_pot += pot;
-          my_g0 += g0;
-          my_g1 += g1;
-          my_g2 += g2;
-        }
-      }
-      if (lane < na) {
-        const int ga = ws.atom[lane];
-        if (dE_dq) dE_dq[ga] += my_pot * pot_scale;
-        if (FORCES) {
-          const T qa = ws.q[lane];
-          const double gx[3] = {-(double)qa * my_g0 * K[0], -(double)qa * my_g1 * K[1], -(double)qa * my_g2 * K[2]};
-          if (dE_dpos) {
-#pragma unroll
-            for (int e = 0; e < 3; ++e) {
-              const double v = gx[0] * g.binv[e * 3 + 0] + gx[1] * g.binv[e * 3 + 1] + gx[2] * g.binv[e * 3 + 2];
-              dE_dpos[3 * (size_t)ga + e] += (T)v;
-            }
-          }
-          const double r[3] = {(double)pos[3 * (size_t)ga], (double)pos[3 * (size_t)ga + 1],
-                               (double)pos[3 * (size_t)ga + 2]};
-#pragma unroll
-          for (int e = 0; e < 3; ++e)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) wf[e * 3 + c] += r[e] * gx[c];
-        }
+        for (int j = j0; j < j1; ++j) brick_column<T>(ws, j, y0, z0, tile, M, d, K1K2);
+        if (j0 + jt < j1) brick_column<T>(ws, j0 + jt, 5, zt, tile, M, d, K1K2);
       }
       __syncwarp();
     }
     __syncthreads();
+    if (!direct) {
+      // add the tile to the mesh, one warp per tile row (consecutive z)
+      for (int r = warp; r < k.ax.w * k.ay.w; r += nw) {
+        const int tx = r / k.ay.w, ty = r - tx * k.ay.w;
+        T* row = M + (size_t)tile_mesh(k.ax, tx) * K1K2 + (size_t)tile_mesh(k.ay, ty) * d.K2;
+        const T* src = tile + (size_t)r * k.az.w;
+        for (int tz = lane; tz < k.az.w; tz += 32) {
+          const T v = src[tz];
+          if (v != T(0)) atomicAdd(row + tile_mesh(k.az, tz), v);
+        }
+      }
+      __syncthreads();
+    }
   }
-  if (FORCES) block_atomic_sum<9>(wf, acc + (size_t)s * kAccStride + kAccWf, red);
 }
 
 }  // namespace admp

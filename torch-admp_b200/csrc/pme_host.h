@@ -233,16 +233,16 @@ inline double plan_atoms(const RecipPlan<T>& p) {
 }
 
 // Atoms binned in cells (order = the cell-sorted atoms, cells = the per-slot
-// cell tables) take the brick-privatised spread / gather; otherwise the
-// direct kernels.
+// cell tables) take the brick-privatised spread; otherwise (and for every
+// gather, whose mesh reads already hit L1 in cell order) the direct kernels.
 template <typename T>
 inline int launch_spread(const Batch& b, const T* pos, const T* box, const T* q, T* mesh, const int* order,
                          const int* cells, int cell_stride, cudaStream_t st) {
   if (!b.nblk_atom) return ADMP_OK;
   if (cells && order) {
-    ADMP_CUDA_TRY(ensure_smem(spread_brick_kernel<T>, brick_smem<T, false>()));
-    spread_brick_kernel<T><<<b.nblk_atom, 256, brick_smem<T, false>(), st>>>(b, pos, box, q, mesh, order, cells,
-                                                                            cell_stride);
+    ADMP_CUDA_TRY(ensure_smem(spread_brick_kernel<T>, brick_smem<T>()));
+    spread_brick_kernel<T><<<b.nblk_atom, 256, brick_smem<T>(), st>>>(b, pos, box, q, mesh, order, cells,
+                                                                     cell_stride);
   } else {
     ADMP_CUDA_TRY(ensure_smem(spread_kernel<T>, spread_smem<T>()));
     spread_kernel<T><<<b.nblk_atom, 256, spread_smem<T>(), st>>>(b, pos, box, q, mesh, order);
@@ -252,18 +252,11 @@ inline int launch_spread(const Batch& b, const T* pos, const T* box, const T* q,
 
 template <typename T, bool F>
 inline int launch_gather(const Batch& b, const T* pos, const T* box, const T* q, const T* phi, T* dE_dq,
-                         T* dE_dpos, double* acc, const int* order, const int* cells, int cell_stride,
-                         cudaStream_t st) {
+                         T* dE_dpos, double* acc, const int* order, cudaStream_t st) {
   if (!b.nblk_atom) return ADMP_OK;
-  if (cells && order) {
-    ADMP_CUDA_TRY(ensure_smem(gather_brick_kernel<T, F>, brick_smem<T, F>()));
-    gather_brick_kernel<T, F><<<b.nblk_atom, 256, brick_smem<T, F>(), st>>>(b, pos, box, q, phi, dE_dq, dE_dpos, acc,
-                                                                           T(1), order, cells, cell_stride);
-  } else {
-    ADMP_CUDA_TRY(ensure_smem(gather_kernel<T, F>, gather_smem<T, F>()));
-    gather_kernel<T, F><<<b.nblk_atom, 256, gather_smem<T, F>(), st>>>(b, pos, box, q, phi, dE_dq, dE_dpos, acc,
-                                                                       T(1), order);
-  }
+  ADMP_CUDA_TRY(ensure_smem(gather_kernel<T, F>, gather_smem<T, F>()));
+  gather_kernel<T, F><<<b.nblk_atom, 256, gather_smem<T, F>(), st>>>(b, pos, box, q, phi, dE_dq, dE_dpos, acc, T(1),
+                                                                     order);
   return ADMP_OK;
 }
 
@@ -282,7 +275,7 @@ inline int launch_recip(const RecipPlan<T>& p, const T* pos, const T* box, const
   s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st);
   if (s) return s;
   h = prof_begin(st);
-  s = launch_gather<T, true>(b, pos, box, q, mesh, dE_dq, dE_dpos, acc, order, cells, cell_stride, st);
+  s = launch_gather<T, true>(b, pos, box, q, mesh, dE_dq, dE_dpos, acc, order, st);
   if (s) return s;
   prof_end(h, PK_GATHER, mb + na * 4 * sizeof(T) + na * 3 * sizeof(T), st);
   count_launches(1);
@@ -306,7 +299,7 @@ inline int launch_recip_potential(const RecipPlan<T>& p, const T* pos, const T* 
   s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st, green);
   if (s) return s;
   h = prof_begin(st);
-  s = launch_gather<T, false>(b, pos, box, v, mesh, pot, nullptr, acc, order, cells, cell_stride, st);
+  s = launch_gather<T, false>(b, pos, box, v, mesh, pot, nullptr, acc, order, st);
   if (s) return s;
   prof_end(h, PK_GATHER, mb + na * 4 * sizeof(T) + na * sizeof(T), st);
   count_launches(2);

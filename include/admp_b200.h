@@ -343,12 +343,6 @@ typedef struct admp_pools {
   double* box64;       /* [S,3,3] or NULL */
   void* frac64;        /* [A] double4 scratch, needed with pos64 */
   int flags;           /* reserved, 0 */
-  /* optional per-slot cell tables written by admp_serve_neighbors: cells per
-   * axis, a valid flag, then the start of each cell's atoms in `sorted`
-   * (cells + 1 entries); with them the reciprocal-space spread and gather
-   * work on bricks of cells in shared memory.  NULL: the direct kernels.    */
-  int* celltab;        /* [S, celltab_stride] */
-  int celltab_stride;  /* ints per slot (>= 5 + cells of the largest system) */
   double* slot_resid;  /* optional [S]: ||P grad||_2 / N of each QEq slot's latest iterate */
 } admp_pools;
 

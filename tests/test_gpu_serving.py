@@ -199,26 +199,3 @@ def test_serving_small_steps_with_backlog_and_call_timeline(cuda, stream_and_ora
     assert all(g["ms"] >= 0.0 for g in tl["largest_gaps"])
     eng.call_trace = None
     assert eng.atoms.used() == 0 and not eng._inflight
-
-
-@pytest.mark.parametrize("dtype,etol,ftol,qtol", [(torch.float64, 1e-10, 1e-8, 1e-9),
-                                                  (torch.float32, 2e-6, 2e-5, 2e-6)])
-def test_brick_spread_gather_match_direct_kernels(cuda, dtype, etol, ftol, qtol):
-    """The brick-privatised spread (cell tables from the neighbour build)
-    against the atom-parallel kernel with global atomics, on systems
-    of 200-20,000 atoms (small boxes whose tiles span the whole period, and
-    large ones with many bricks per system).  PME results agree to rounding;
-    QEq results within the two solves' own convergence (CG to 1e-10 in FP64)."""
-    from admp_b200 import synthetic
-    reqs = synthetic.serving_stream(40, 23, rate=1000.0)
-    reqs = sorted(reqs, key=lambda r: r.natoms)[::4]
-    tol = 1e-10 if dtype == torch.float64 else 1e-7
-    a, _ = serve(reqs, dtype, tol, bricks=True)
-    b, _ = serve(reqs, dtype, tol, bricks=False)
-    for r in reqs:
-        x, y = a[r.rid], b[r.rid]
-        assert x.status == 0 and y.status == 0
-        assert abs(x.energy - y.energy) / abs(y.energy) < etol, (r.kind, r.natoms)
-        assert np.abs(x.forces - y.forces).max() / np.abs(y.forces).max() < ftol, (r.kind, r.natoms)
-        if y.charges is not None:
-            assert np.abs(x.charges - y.charges).max() < qtol, (r.kind, r.natoms)

@@ -57,11 +57,7 @@ class AdmpPools(ctypes.Structure):
                [("mesh_cap", ctypes.c_longlong), ("spec", _P), ("spec_cap", ctypes.c_longlong), ("acc", _P),
                 ("acc_cap", ctypes.c_int), ("cells", _P), ("cells_cap", ctypes.c_longlong), ("sys_scratch", _P),
                 ("sys_scratch_bytes", ctypes.c_longlong), ("green", _P), ("green_cap", ctypes.c_longlong),
-                ("pos64", _P), ("box64", _P), ("frac64", _P), ("flags", ctypes.c_int), ("celltab", _P),
-                ("celltab_stride", ctypes.c_int), ("slot_resid", _P)]
-
-# ints per slot of the cell tables (header + cell starts; systems with more cells use the direct kernels)
-CELLTAB_STRIDE = 1024
+                ("pos64", _P), ("box64", _P), ("frac64", _P), ("flags", ctypes.c_int), ("slot_resid", _P)]
 
 _COPY_THREADS = 4  # host threads copying request arrays into the pinned staging buffers
 
@@ -168,8 +164,7 @@ class ServingEngine:
     def __init__(self, device="cuda:0", dtype=torch.float32, max_atoms: int = 4_000_000, max_slots: int = 512,
                  pairs_per_atom: float = 150.0, mesh_budget: int = 64_000_000, rcut: float = 6.0,
                  ethresh: float = 5e-4, tol: float = 1e-6, max_iter: int = 300, iters_per_tick: int = 8,
-                 ke: float = DIELECTRIC, green_budget: Optional[int] = None, admit_per_tick: int = 512,
-                 bricks: bool = True):
+                 ke: float = DIELECTRIC, green_budget: Optional[int] = None, admit_per_tick: int = 512):
         self.lib = L.load()
         _bind_serve(self.lib)
         self.dev = torch.device(device)
@@ -205,7 +200,6 @@ class ServingEngine:
             "sys_scratch": torch.zeros(self.lib.admp_serve_sys_scratch_bytes(MAX_PER_LAUNCH), dtype=torch.uint8,
                                        device=self.dev),
             "green": torch.zeros(green_budget if green_budget is not None else mesh_budget, **f),
-            "celltab": torch.zeros(max_slots * CELLTAB_STRIDE, **i32),
             "slot_resid": torch.zeros(max_slots, **f64),
         }
         if dtype == torch.float32:
@@ -228,10 +222,6 @@ class ServingEngine:
         self.pools.sys_scratch_bytes = t["sys_scratch"].numel()
         self.pools.green_cap = t["green"].numel()
         self.pools.flags = 0
-        # reciprocal-space spread / gather on bricks of neighbour cells in shared memory (the cell tables
-        # come from the neighbour build); bricks=False keeps the atom-parallel kernels with global atomics
-        self.pools.celltab = t["celltab"].data_ptr() if bricks else None
-        self.pools.celltab_stride = CELLTAB_STRIDE
         self.pools.slot_resid = t["slot_resid"].data_ptr()
         self.greens = _Intervals(t["green"].numel(), 32)
         self.mesh_budget = mesh_budget

@@ -3,7 +3,6 @@
 
 #include <vector>
 
-#include "brick_kernels.cuh"
 #include "pme_kernels.cuh"
 #include "runtime.h"
 
@@ -232,21 +231,12 @@ inline double plan_atoms(const RecipPlan<T>& p) {
   return n;
 }
 
-// Atoms binned in cells (order = the cell-sorted atoms, cells = the per-slot
-// cell tables) take the brick-privatised spread; otherwise (and for every
-// gather, whose mesh reads already hit L1 in cell order) the direct kernels.
 template <typename T>
 inline int launch_spread(const Batch& b, const T* pos, const T* box, const T* q, T* mesh, const int* order,
-                         const int* cells, int cell_stride, cudaStream_t st) {
+                         cudaStream_t st) {
   if (!b.nblk_atom) return ADMP_OK;
-  if (cells && order) {
-    ADMP_CUDA_TRY(ensure_smem(spread_brick_kernel<T>, brick_smem<T>()));
-    spread_brick_kernel<T><<<b.nblk_atom, 256, brick_smem<T>(), st>>>(b, pos, box, q, mesh, order, cells,
-                                                                     cell_stride);
-  } else {
-    ADMP_CUDA_TRY(ensure_smem(spread_kernel<T>, spread_smem<T>()));
-    spread_kernel<T><<<b.nblk_atom, 256, spread_smem<T>(), st>>>(b, pos, box, q, mesh, order);
-  }
+  ADMP_CUDA_TRY(ensure_smem(spread_kernel<T>, spread_smem<T>()));
+  spread_kernel<T><<<b.nblk_atom, 256, spread_smem<T>(), st>>>(b, pos, box, q, mesh, order);
   return ADMP_OK;
 }
 
@@ -263,12 +253,12 @@ inline int launch_gather(const Batch& b, const T* pos, const T* box, const T* q,
 template <typename T>
 inline int launch_recip(const RecipPlan<T>& p, const T* pos, const T* box, const T* q, T* mesh, Cplx<T>* spec,
                         double* acc, double ke, T* dE_dq, T* dE_dpos, cudaStream_t st,
-                        const int* order = nullptr, const int* cells = nullptr, int cell_stride = 0) {
+                        const int* order = nullptr) {
   const Batch& b = p.b;
   const double na = plan_atoms(p), mb = (double)p.mesh_elems * sizeof(T);
   ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
   int h = prof_begin(st);
-  int s = launch_spread<T>(b, pos, box, q, mesh, order, cells, cell_stride, st);
+  int s = launch_spread<T>(b, pos, box, q, mesh, order, st);
   if (s) return s;
   prof_end(h, PK_SPREAD, na * 4 * sizeof(T) + mb, st);
   count_launches(1);
@@ -287,13 +277,12 @@ inline int launch_recip(const RecipPlan<T>& p, const T* pos, const T* box, const
 template <typename T>
 inline int launch_recip_potential(const RecipPlan<T>& p, const T* pos, const T* box, const T* v, T* mesh,
                                   Cplx<T>* spec, double* acc, double ke, T* pot, cudaStream_t st,
-                                  const int* order = nullptr, const T* green = nullptr, const int* cells = nullptr,
-                                  int cell_stride = 0) {
+                                  const int* order = nullptr, const T* green = nullptr) {
   const Batch& b = p.b;
   const double na = plan_atoms(p), mb = (double)p.mesh_elems * sizeof(T);
   ADMP_CUDA_TRY(cudaMemsetAsync(mesh, 0, p.mesh_elems * sizeof(T), st));
   int h = prof_begin(st);
-  int s = launch_spread<T>(b, pos, box, v, mesh, order, cells, cell_stride, st);
+  int s = launch_spread<T>(b, pos, box, v, mesh, order, st);
   if (s) return s;
   prof_end(h, PK_SPREAD, na * 4 * sizeof(T) + mb, st);
   s = launch_fft_green<T>(p, mesh, spec, box, acc, ke, st, green);

@@ -178,10 +178,6 @@ static int serve_neighbors_impl(const admp_pools* P, const admp_sys* sys, int ns
                                                 P->pos64 ? (double4*)P->frac64 : nullptr, P->cell_of, P->cells,
                                                 P->pcnt, P->pstart);
   sn_scan_cells_kernel<<<nsys, 1024, 0, st>>>(ss, P->cells);
-  if (P->celltab) {
-    sn_celltab_kernel<<<nsys, 256, 0, st>>>(b, ss, P->cells, P->celltab, P->celltab_stride);
-    count_launches(1);
-  }
   sn_scatter_kernel<<<b.nblk_atom, 256, 0, st>>>(b, ss, P->cell_of, P->cells, P->sorted);
   sn_pairs_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, ss, (const V4*)P->frac, f64, P->cell_of, P->cells, P->sorted,
                                                   P->pcnt, P->pstart, P->col);
@@ -212,7 +208,7 @@ static int serve_ef_impl(const admp_pools* P, const admp_sys* sys, int nsys, dou
   count_launches(6);
   ADMP_CUDA_TRY(cudaMemsetAsync(P->acc, 0, sizeof(double) * kAccStride * nsys, st));
   s = launch_recip<T>(plan, (const T*)P->pos, (const T*)P->box, (const T*)P->q, (T*)P->mesh, (Cplx<T>*)P->spec,
-                      P->acc, ke, nullptr, (T*)P->force, st, P->sorted, P->celltab, P->celltab_stride);
+                      P->acc, ke, nullptr, (T*)P->force, st, P->sorted);
   if (s) return s;
   recip_finalize_kernel<T><<<(nsys + 127) / 128, 128, 0, st>>>(b, (const T*)P->box, P->acc, P->energy, nullptr);
   sys_terms_kernel<T><<<nsys, 512, 0, st>>>(b, ss, (const T*)P->q, (const T*)P->chi, (const T*)P->hardness,
@@ -311,8 +307,7 @@ static int srv_matvec(const admp_pools* P, const RecipPlan<T>& plan, QEqParams p
                       double* hv_out, double ke, cudaStream_t st) {
   const Batch& b = plan.b;
   int s = launch_recip_potential<T>(plan, (const T*)P->pos, (const T*)P->box, v, (T*)P->mesh, (Cplx<T>*)P->spec,
-                                    P->acc, ke, Hv, st, P->sorted, (const T*)P->green, P->celltab,
-                                    P->celltab_stride);
+                                    P->acc, ke, Hv, st, P->sorted, (const T*)P->green);
   if (s) return s;
   int h = prof_begin(st);
   csr_spmv_finish_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, P->pstart, P->pcnt, P->col, (const T*)P->coef, v,

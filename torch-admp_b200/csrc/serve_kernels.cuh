@@ -8,7 +8,6 @@
 //   sys_terms : per-system self / non-neutral / damping-self / site energies
 #pragma once
 
-#include "brick_kernels.cuh"
 #include "pme_kernels.cuh"
 
 namespace admp {
@@ -162,26 +161,6 @@ static __global__ void sn_scan_cells_kernel(SrvSys* __restrict__ ss, int* __rest
     start[i] = acc;
     acc += cnt[i];
   }
-}
-
-// block per system: the cell table of its slot (cells per axis, valid flag,
-// cell starts in the cell-sorted order), read by the brick spread / gather
-static __global__ void __launch_bounds__(256)
-    sn_celltab_kernel(Batch b, const SrvSys* __restrict__ ss, const int* __restrict__ cells, int* __restrict__ tab,
-                      int stride) {
-  const SrvSys& S = ss[blockIdx.x];
-  int* t = tab + (size_t)b.s[blockIdx.x].box_idx * stride;
-  const int n = S.ncells;
-  const bool ok = S.status == 0 && n > 0 && n + 1 + kCellHdr <= stride;
-  if (threadIdx.x == 0) {
-    t[0] = S.nc[0];
-    t[1] = S.nc[1];
-    t[2] = S.nc[2];
-    t[3] = ok ? 1 : 0;
-  }
-  if (!ok) return;
-  const int* start = cells + S.cell_off + (n + 1);
-  for (int c = threadIdx.x; c <= n; c += blockDim.x) t[kCellHdr + c] = start[c];
 }
 
 static __global__ void __launch_bounds__(256)

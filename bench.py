@@ -433,6 +433,27 @@ def electrode_leg(dev):
             r["max_charge_err_vs_reference_e"] = float(np.abs(q - g["q_ref"]).max())
             r["rel_energy_err_vs_reference"] = abs(E - float(g["E"])) / abs(float(g["E"]))
         out[tag] = r
+    # the dense path (method="matinv": Hessian from batched Hessian-vector products + KKT solve), FP64
+    calc = PolarizableElectrode(rcut=RCUT, ethresh=ETHRESH, kmesh=[64, 64, 160], slab_corr=True, eps=1e-10,
+                                max_iter=2000)
+    pos = torch.tensor(pos_np, dtype=torch.float64, device=dev, requires_grad=True)
+    box = torch.tensor(box_np, dtype=torch.float64, device=dev)
+    ch = torch.tensor(q_np, dtype=torch.float64, device=dev)
+    nb = TorchNeighborList(RCUT)
+    pairs = nb(pos, box)
+    cons = [LAMMPSElectrodeConstraint(indices=top, value=1.0, mode="conp", eta=math.sqrt(2.0)),
+            LAMMPSElectrodeConstraint(indices=bot, value=0.0, mode="conp", eta=math.sqrt(2.0))]
+    data = setup_from_lammps(len(q_np), cons, True, device=dev, dtype=torch.float64)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    E, F, q = infer(calc, pos, box, ch, pairs, nb.get_ds(), nb.get_buffer_scales(), *data, method="matinv")
+    torch.cuda.synchronize()
+    r = {"ms": (time.perf_counter() - t0) * 1e3}
+    if g is not None:
+        r["max_charge_err_vs_reference_e"] = float(np.abs(q.detach().cpu().numpy() - g["q_ref"]).max())
+    out["fp64_matinv"] = r
+    del pos, box, ch, pairs, nb, data, E, F, q
+    torch.cuda.empty_cache()
     if g is not None:
         out["reference_cpu_s"] = float(g["time_ref_s"])
         out["reference_cpu_note"] = (f"the reference's infer(method='lbfgs', eps 1e-8) on {int(g['threads'])} CPU "

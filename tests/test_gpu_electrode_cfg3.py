@@ -15,7 +15,7 @@ from _gpu_helpers import T, rel
 pytestmark = pytest.mark.gpu
 
 
-def _run(cuda, dtype, eps):
+def _run(cuda, dtype, eps, method="lbfgs"):
     from admp_b200 import synthetic
     from admp_b200.electrode import LAMMPSElectrodeConstraint, PolarizableElectrode, infer, setup_from_lammps
     from admp_b200.nblist import TorchNeighborList
@@ -33,7 +33,7 @@ def _run(cuda, dtype, eps):
     cons = [LAMMPSElectrodeConstraint(indices=np.arange(int(a), int(z)), value=float(v), mode="conp",
                                       eta=float(d["lammps_eta"])) for a, z, v, _ in d["cons"]]
     data = setup_from_lammps(len(q_np), cons, True, device=cuda, dtype=dtype)
-    E, F, q = infer(calc, pos, box, charges, pairs, nb.get_ds(), nb.get_buffer_scales(), *data, method="lbfgs")
+    E, F, q = infer(calc, pos, box, charges, pairs, nb.get_ds(), nb.get_buffer_scales(), *data, method=method)
     torch.cuda.synchronize()
     mask = data[0].cpu().numpy()
     return d, float(E), F.detach().double().cpu().numpy(), q.detach().double().cpu().numpy(), mask, calc
@@ -57,3 +57,14 @@ def test_electrode_cfg3_fp32_within_stated_error(cuda):
     assert rel(F, d["forces"]) < 1e-4
     assert np.abs(q - d["q_ref"]).max() < 1e-5
     assert abs(E - float(d["E"])) / abs(float(d["E"])) < 1e-5
+
+
+def test_electrode_cfg3_dense_kkt_matches_reference(cuda):
+    """method="matinv": the 2,304 x 2,304 electrode Hessian from batched
+    Hessian-vector products (64 unit vectors per call) and the dense KKT solve
+    give the reference's charges and forces as well."""
+    d, E, F, q, mask, calc = _run(cuda, torch.float64, 1e-10, method="matinv")
+    assert abs(E - float(d["E"])) / abs(float(d["E"])) < 1e-8
+    assert rel(F, d["forces"]) < 1e-6
+    assert np.abs(q - d["q_ref"]).max() / np.abs(d["q_ref"]).max() < 2e-6
+    assert abs(q[mask].sum()) < 1e-9

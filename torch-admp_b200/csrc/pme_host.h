@@ -57,6 +57,19 @@ inline int bind_plan(RecipPlan<T>& p, SysDesc* dev, cudaStream_t st) {
   return ADMP_OK;
 }
 
+// The plan's launch descriptor with the first-block column of family F
+// (F_ATOM is the plan's own; the FFT passes take theirs at their launches).
+template <typename T>
+inline Batch family_batch(const RecipPlan<T>& p, int F) {
+  Batch b = p.b;
+  b.fam = F;
+  for (int s = 0; s < b.nsys; ++s) {
+    const SysDesc& d = p.hs[s];
+    b.blk[s] = F == F_ATOM ? d.blk_atom : F == F_Z ? d.blk_z : F == F_Y ? d.blk_y : F == F_X ? d.blk_x : d.blk_slab;
+  }
+  return b;
+}
+
 // device bytes of a system table (kept 256-byte aligned for what follows it)
 inline size_t sys_table_bytes() { return align_up(sizeof(SysDesc) * kMaxBatch, 256); }
 
@@ -146,6 +159,8 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
     const int ppb = slab_ppb(be, slab_plane_elems(sys[s].K[1], sys[s].K[2]), sys[s].K[0]);
     b.nblk_slab += (sys[s].K[0] + ppb - 1) / ppb;
   }
+  b.fam = F_ATOM;
+  for (int s = 0; s < nsys; ++s) b.blk[s] = p.hs[s].blk_atom;
   return ADMP_OK;
 }
 
@@ -153,7 +168,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
 // 2 G_s for every half-spectrum point of the batch, at each system's green_off
 template <typename T>
 inline int launch_green_build(const RecipPlan<T>& p, const T* box, T* green, double ke, cudaStream_t st) {
-  if (p.b.nblk_x) green_build_kernel<T><<<p.b.nblk_x, 256, 0, st>>>(p.b, box, green, ke);
+  if (p.b.nblk_x) green_build_kernel<T><<<p.b.nblk_x, 256, 0, st>>>(family_batch(p, F_X), box, green, ke);
   count_launches(1);
   ADMP_CUDA_TRY(cudaGetLastError());
   return ADMP_OK;
@@ -163,6 +178,8 @@ template <typename T>
 inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const T* box, double* acc, double ke,
                             cudaStream_t st, const T* green = nullptr) {
   const Batch& b = p.b;
+  const Batch bsl = family_batch(p, F_SLAB), bz = family_batch(p, F_Z), by = family_batch(p, F_Y),
+              bx = family_batch(p, F_X);
   ADMP_CUDA_TRY(ensure_smem(fft_z_fwd_kernel<T>, p.smem_z));
   ADMP_CUDA_TRY(ensure_smem(fft_z_inv_kernel<T>, p.smem_z));
   ADMP_CUDA_TRY(ensure_smem(fft_y_kernel<T, false>, p.smem_y));
@@ -176,36 +193,36 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
     ADMP_CUDA_TRY(ensure_smem(fft_slab_fwd_kernel<T>, p.smem_slab));
     ADMP_CUDA_TRY(ensure_smem(fft_slab_inv_kernel<T>, p.smem_slab));
     h = prof_begin(st);
-    if (b.nblk_slab) fft_slab_fwd_kernel<T><<<b.nblk_slab, 256, p.smem_slab, st>>>(b, mesh, spec, p.buf_elems);
+    if (b.nblk_slab) fft_slab_fwd_kernel<T><<<b.nblk_slab, 256, p.smem_slab, st>>>(bsl, mesh, spec, p.buf_elems);
     prof_end(h, PK_FFT_Z_FWD, rb + cb, st);
   } else {
     h = prof_begin(st);
-    if (b.nblk_z) fft_z_fwd_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, mesh, spec);
+    if (b.nblk_z) fft_z_fwd_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(bz, mesh, spec);
     prof_end(h, PK_FFT_Z_FWD, rb + cb, st);
     h = prof_begin(st);
-    if (b.nblk_y) fft_y_kernel<T, false><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
+    if (b.nblk_y) fft_y_kernel<T, false><<<b.nblk_y, 256, p.smem_y, st>>>(by, spec);
     prof_end(h, PK_FFT_Y_FWD, 2 * cb, st);
   }
   h = prof_begin(st);
   if (b.nblk_x) {
     if (green)
-      fft_x_apply_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(b, spec, green);
+      fft_x_apply_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(bx, spec, green);
     else
-      fft_x_green_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(b, spec, box, acc, ke);
+      fft_x_green_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(bx, spec, box, acc, ke);
   }
   // spectrum in and out, plus the cached Green's function (one real per entry) when it is read
   prof_end(h, PK_FFT_X_GREEN, 2 * cb + (green ? (double)p.spec_elems * sizeof(T) : 0.0), st);
   if (p.slab) {
     h = prof_begin(st);
-    if (b.nblk_slab) fft_slab_inv_kernel<T><<<b.nblk_slab, 256, p.smem_slab, st>>>(b, spec, mesh, p.buf_elems);
+    if (b.nblk_slab) fft_slab_inv_kernel<T><<<b.nblk_slab, 256, p.smem_slab, st>>>(bsl, spec, mesh, p.buf_elems);
     prof_end(h, PK_FFT_Z_INV, rb + cb, st);
     count_launches(3);
   } else {
     h = prof_begin(st);
-    if (b.nblk_y) fft_y_kernel<T, true><<<b.nblk_y, 256, p.smem_y, st>>>(b, spec);
+    if (b.nblk_y) fft_y_kernel<T, true><<<b.nblk_y, 256, p.smem_y, st>>>(by, spec);
     prof_end(h, PK_FFT_Y_INV, 2 * cb, st);
     h = prof_begin(st);
-    if (b.nblk_z) fft_z_inv_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(b, spec, mesh);
+    if (b.nblk_z) fft_z_inv_kernel<T><<<b.nblk_z, 256, p.smem_z, st>>>(bz, spec, mesh);
     prof_end(h, PK_FFT_Z_INV, rb + cb, st);
     count_launches(5);
   }

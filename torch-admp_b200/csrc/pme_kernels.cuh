@@ -43,6 +43,12 @@ struct Batch {
   const int* done;   // optional per-slot skip flags (done[slot * done_stride], slot = box_idx)
   int done_stride;
   const SysDesc* s;  // device table [nsys]
+  // first block of every system in the block family `fam` of this launch (a
+  // copy of the table's blk_* column, ~1 KB): a block finds its system by
+  // binary search over this parameter array (constant bank, broadcast)
+  // instead of a chain of dependent global loads into the table
+  int fam;
+  int blk[kMaxBatch];
 };
 
 __device__ __forceinline__ bool skip_sys(const Batch& b, int s) {
@@ -66,8 +72,18 @@ __device__ __forceinline__ int blk_of(const SysDesc& d) {
 template <int F>
 __device__ __forceinline__ int find_sys(const Batch& b, int blk) {
   int lo = 0, hi = b.nsys - 1;
+  if (b.fam == F) {
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (b.blk[mid] <= blk)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    return lo;
+  }
   while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
+    const int mid = (lo + hi + 1) >> 1;
     if (blk_of<F>(b.s[mid]) <= blk)
       lo = mid;
     else
@@ -242,7 +258,7 @@ __global__ void __launch_bounds__(256) spread_kernel(Batch b, const T* __restric
   __shared__ Geom g;
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc& d = b.s[s];  // a register copy would cost this kernel 10 registers
   load_geom(box, d.box_idx, &g);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -296,7 +312,7 @@ __global__ void __launch_bounds__(256) fft_z_fwd_kernel(Batch b, const T* __rest
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int s = find_sys<F_Z>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int K2 = d.K2, K2h = d.K2h, L = d.K0 * d.K1, npair = (L + 1) / 2;
   const FastDiv fdK2 = fast_div(K2), fdK2h = fast_div(K2h);
   const int p0 = (blockIdx.x - d.blk_z) * b.lp;
@@ -340,7 +356,7 @@ __global__ void __launch_bounds__(256) fft_y_kernel(Batch b, Cplx<T>* __restrict
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int s = find_sys<F_Y>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int K1 = d.K1, K2h = d.K2h, zb = b.zb;
   const int ncb = (K2h + zb - 1) / zb;
   const int local = blockIdx.x - d.blk_y;
@@ -376,7 +392,7 @@ __global__ void __launch_bounds__(256) fft_x_green_kernel(Batch b, Cplx<T>* __re
   __shared__ double red[10 * 32];
   const int s = find_sys<F_X>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h, zb = b.zb;
   // this block: columns [c0, c0 + nz) of the flattened (y, kz) index c = y K2h + kz
   const int c0 = (blockIdx.x - d.blk_x) * zb, nz = min(zb, K1 * K2h - c0);
@@ -509,7 +525,7 @@ __global__ void __launch_bounds__(256) fft_slab_fwd_kernel(Batch b, const T* __r
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int s = find_sys<F_SLAB>(b, blockIdx.x);  // a block per run of x planes
   if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h;
   const int np = (K1 + 1) / 2;
   const int ppb = slab_ppb(buf_elems, slab_plane_elems(K1, K2), K0);
@@ -569,7 +585,7 @@ __global__ void __launch_bounds__(256) fft_slab_inv_kernel(Batch b, const Cplx<T
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int s = find_sys<F_SLAB>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h;
   const int np = (K1 + 1) / 2;
   const int ppb = slab_ppb(buf_elems, slab_plane_elems(K1, K2), K0);
@@ -639,7 +655,7 @@ __global__ void __launch_bounds__(256) green_build_kernel(Batch b, const T* __re
                                                           double ke) {
   __shared__ Geom g;
   const int s = find_sys<F_X>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2 = d.K2, K2h = d.K2h, zb = b.zb;
   const int c0 = (blockIdx.x - d.blk_x) * zb, nz = min(zb, K1 * K2h - c0);
   const FastDiv fdnz = fast_div(nz);
@@ -677,7 +693,7 @@ __global__ void __launch_bounds__(256) fft_x_apply_kernel(Batch b, Cplx<T>* __re
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int s = find_sys<F_X>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int K0 = d.K0, K1 = d.K1, K2h = d.K2h, zb = b.zb;
   // this block: columns [c0, c0 + nz) of the flattened (y, kz) index c = y K2h + kz
   const int c0 = (blockIdx.x - d.blk_x) * zb, nz = min(zb, K1 * K2h - c0);
@@ -732,7 +748,7 @@ __global__ void __launch_bounds__(256) fft_z_inv_kernel(Batch b, const Cplx<T>* 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int s = find_sys<F_Z>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int K2 = d.K2, K2h = d.K2h, L = d.K0 * d.K1, npair = (L + 1) / 2;
   const FastDiv fdK2 = fast_div(K2);
   const int p0 = (blockIdx.x - d.blk_z) * b.lp;
@@ -792,7 +808,7 @@ __global__ void __launch_bounds__(256) gather_kernel(Batch b, const T* __restric
   __shared__ double red[9 * 32];
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   if (skip_sys(b, s)) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   load_geom(box, d.box_idx, &g);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -936,7 +952,7 @@ __global__ void recip_finalize_kernel(Batch b, const T* __restrict__ box, const 
                                       double* __restrict__ energy, T* __restrict__ dE_dbox) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= b.nsys) return;
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   double bx[9], bi[9];
   load_box(box + (size_t)d.box_idx * 9, bx);
   inv3(bx, bi);

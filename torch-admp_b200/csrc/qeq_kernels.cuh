@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(256)
                      const T* __restrict__ shift, double* __restrict__ diag, double* __restrict__ zc,
                      double* __restrict__ chi_eff, CGScal* __restrict__ sc) {
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s0];
+  const SysDesc d = b.s[s0];
   const int s = d.box_idx;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256)
     qeq_gram_kernel(Batch b, int nc, const T* __restrict__ C, long long cstride, CGScal* __restrict__ sc) {
   __shared__ double red[16 * 32];
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s0];
+  const SysDesc d = b.s[s0];
   const int s = d.box_idx;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256)
                     T* __restrict__ vt) {
   __shared__ double red[7 * 32];
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s0];
+  const SysDesc d = b.s[s0];
   const int s = d.box_idx;
   if (sys_done<T>(sc, s)) return;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(256)
                       long long cstride, CGScal* __restrict__ sc, double* __restrict__ hv_out) {
   __shared__ double red[5 * 32];
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s0];
+  const SysDesc d = b.s[s0];
   const int s = d.box_idx;
   if (sc[s].done) return;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256)
                       T* __restrict__ Hp, const T* __restrict__ C, long long cstride, CGScal* __restrict__ sc) {
   __shared__ double red[32];
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s0];
+  const SysDesc d = b.s[s0];
   const int s = d.box_idx;
   if (sc[s].done) return;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(256)
                          const double* __restrict__ zc, CGScal* __restrict__ sc) {
   __shared__ double red[3 * 32];
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s0];
+  const SysDesc d = b.s[s0];
   const int s = d.box_idx;
   if (sc[s].done) return;
   const CGScal& S = sc[s];
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(256)
     qeq_project_kernel(Batch b, double* __restrict__ x, const T* __restrict__ C, long long cstride,
                        const CGScal* __restrict__ sc) {
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s0];
+  const SysDesc d = b.s[s0];
   const int s = d.box_idx;
   const CGScal& S = sc[s];
   const int nc = S.n_const;
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(256)
                      double* __restrict__ r, T* __restrict__ p, CGScal* __restrict__ sc, int pass) {
   __shared__ double red[4 * 32];
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s0];
+  const SysDesc d = b.s[s0];
   const int s = d.box_idx;
   const CGScal& S = sc[s];
   const int nc = S.n_const;

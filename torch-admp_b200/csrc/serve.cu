@@ -22,7 +22,7 @@ __global__ void srv_table_kernel(SrvLaunch L, const void* box_v, int dbl, const 
                                  SrvSys* __restrict__ ss, int fresh) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= L.b.nsys) return;
-  const SysDesc& d = L.b.s[s];
+  const SysDesc d = L.b.s[s];
   SrvSys& S = ss[s];
   S.pair_off = L.pair_off[s];
   S.pair_cap = L.pair_cap[s];
@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(256) cast_atoms_kernel(Batch b, const T* __res
                                                          int to_double, T* __restrict__ back,
                                                          const double* __restrict__ src) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) cast_atoms_kernel(Batch b, const T* __res
 template <typename T>
 __global__ void __launch_bounds__(256) zero_vec_kernel(Batch b, T* __restrict__ v) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) v[d.atom_off + a] = T(0);
@@ -230,7 +230,7 @@ static __global__ void __launch_bounds__(256)
                            CGScal* __restrict__ sc, double* __restrict__ hv_out) {
   __shared__ double red[5 * 32];
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s0];
+  const SysDesc d = b.s[s0];
   const int s = d.box_idx;
   if (sc[s].done) return;
   const CGScal& S = sc[s];

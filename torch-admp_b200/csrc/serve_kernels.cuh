@@ -97,7 +97,7 @@ static __global__ void __launch_bounds__(256)
                   typename Vec4<T>::type* __restrict__ frac, double4* __restrict__ frac64, int* __restrict__ cell_of,
                   int* __restrict__ cells, int* __restrict__ pcnt, long long* __restrict__ pstart) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const SrvSys& S = ss[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
@@ -167,7 +167,7 @@ static __global__ void __launch_bounds__(256)
     sn_scatter_kernel(Batch b, const SrvSys* __restrict__ ss, const int* __restrict__ cell_of, int* __restrict__ cells,
                       int* __restrict__ sorted) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const SrvSys& S = ss[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
@@ -254,7 +254,7 @@ static __global__ void __launch_bounds__(256)
   __shared__ int cand_j[8][2][32];
   __shared__ int tb_begin[8][27], tb_end[8][27], tb_shift[8][27];
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   SrvSys& S = ss[s];
   if (S.status) return;  // sn_bin_kernel left every count of a failed system at zero
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -470,7 +470,7 @@ static __global__ void __launch_bounds__(256)
   __shared__ double bx[9];
   __shared__ double red[32];
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const SrvSys& S = ss[s];
   if (threadIdx.x < 9) bx[threadIdx.x] = S.b[threadIdx.x];
   __syncthreads();
@@ -569,7 +569,7 @@ static __global__ void __launch_bounds__(256)
                     const int* __restrict__ col, double ke, T* __restrict__ coef) {
   __shared__ double bx[9];
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const SrvSys& S = ss[s];
   if (threadIdx.x < 9) bx[threadIdx.x] = S.b[threadIdx.x];
   __syncthreads();
@@ -627,7 +627,7 @@ __global__ void __launch_bounds__(512)
                      const T* __restrict__ hard, const T* __restrict__ eta, double ke, double* __restrict__ energy) {
   __shared__ double red[4 * 32];
   __shared__ double sums[4];
-  const SysDesc& d = b.s[blockIdx.x];
+  const SysDesc d = b.s[blockIdx.x];
   const SrvSys& S = ss[blockIdx.x];
   if (threadIdx.x < 4) sums[threadIdx.x] = 0.0;
   __syncthreads();
@@ -658,7 +658,7 @@ __global__ void __launch_bounds__(512)
 template <typename T>
 __global__ void __launch_bounds__(256) zero_atoms_kernel(Batch b, T* __restrict__ a3, double* __restrict__ energy) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
@@ -673,7 +673,7 @@ __global__ void __launch_bounds__(256) zero_atoms_kernel(Batch b, T* __restrict_
 template <typename T>
 __global__ void __launch_bounds__(256) negate_atoms_kernel(Batch b, T* __restrict__ a3) {
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
-  const SysDesc& d = b.s[s];
+  const SysDesc d = b.s[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {

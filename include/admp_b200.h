@@ -314,7 +314,7 @@ typedef struct admp_pools {
   int* cell_of;        /* [A]   scratch */
   int* sorted;         /* [A]   scratch */
   /* per pair */
-  unsigned short* col; /* [P]   neighbour atom: index within its system (systems of at most 65535 atoms) */
+  int* col;            /* [P]   neighbour atom (pool index) */
   void* coef;          /* [P]   QEq real-space matrix entries (dtype) */
   /* per slot */
   void* box;           /* [S,3,3] */

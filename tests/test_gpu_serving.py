@@ -215,14 +215,3 @@ def test_run_to_run_spread(cuda, stream_and_oracle):
                  for r in reqs)
         print(f"run-to-run {dtype}: energy {de:.2e}, force {df:.2e}")
         assert de < etol and df < ftol, (dtype, de, df)
-
-
-def test_serving_rejects_systems_beyond_16bit_columns(cuda):
-    """Neighbour columns are 16-bit indices within a system: a request of more
-    than 65535 atoms is refused at submission, before anything is launched."""
-    from admp_b200.serving import ServingEngine
-    from admp_b200.synthetic import Request
-    eng = ServingEngine(dtype=torch.float32, max_atoms=10_000, max_slots=4, mesh_budget=1_000_000)
-    big = Request(0, "pme", 0.0, np.zeros((65536, 3)), np.eye(3) * 90.0, charges=np.zeros(65536))
-    with pytest.raises(ValueError, match="at most 65535 atoms"):
-        eng.submit(big)

@@ -38,7 +38,6 @@ from .utils import DIELECTRIC
 
 SYS_PME, SYS_QEQ = 0, 1
 MAX_PER_LAUNCH = 256
-MAX_SERVE_ATOMS = 65535
 
 
 class AdmpSys(ctypes.Structure):
@@ -187,7 +186,7 @@ class ServingEngine:
             "hardness": torch.zeros(A, **f), "eta": torch.zeros(A, **f), "force": torch.zeros(A, 3, **f),
             "frac": torch.zeros(A, 4, **f), "pstart": torch.zeros(A, dtype=torch.int64, device=self.dev),
             "pcnt": torch.zeros(A, **i32), "cell_of": torch.zeros(A, **i32), "sorted": torch.zeros(A, **i32),
-            "col": torch.zeros(Pn, dtype=torch.int16, device=self.dev), "coef": torch.zeros(Pn, **f),
+            "col": torch.zeros(Pn, **i32), "coef": torch.zeros(Pn, **f),
             "box": torch.zeros(max_slots, 3, 3, **f), "energy": torch.zeros(max_slots, **f64),
             "cg_state": torch.zeros(max_slots * self.lib.admp_serve_slot_state_bytes(), dtype=torch.uint8,
                                     device=self.dev),
@@ -276,16 +275,13 @@ class ServingEngine:
         """Device bytes a request holds while resident (atoms, pairs) and its mesh scratch."""
         fb = 4 if self.dtype == torch.float32 else 8
         per_atom = fb * 17 + 8 * 7 + 4 * 3
-        per_pair = 2 + fb
+        per_pair = 4 + fb
         km = auto_kmesh(np.diagonal(self._box_host(req)), self.kappa, self.ethresh)
         return {"atom_bytes": req.natoms * per_atom, "pair_bytes": self._pair_estimate(req) * per_pair,
                 "mesh_elems": self._mesh_of(km)}
 
     # -- API ------------------------------------------------------------------
     def submit(self, req, t_arrival: Optional[float] = None) -> None:
-        if req.natoms > MAX_SERVE_ATOMS:
-            raise ValueError(f"serving systems hold at most {MAX_SERVE_ATOMS} atoms (neighbour columns are 16-bit "
-                             f"indices within the system), got {req.natoms}")
         self.queue.append((req, time.perf_counter() if t_arrival is None else t_arrival))
 
     def _facts(self, req):

@@ -124,9 +124,6 @@ static int srv_build(const admp_pools* P, const admp_sys* sys, int nsys, RecipPl
   for (int s = 0; s < nsys; ++s) {
     const admp_sys& a = sys[s];
     if (a.natoms <= 0 || a.atom_off < 0 || a.slot < 0) return fail(ADMP_ERR_BAD_ARG, "serve: bad system %d", s);
-    if (a.natoms > kMaxServeAtoms)
-      return fail(ADMP_ERR_BAD_ARG, "serve: system %d has %d atoms (at most %d per served system)", s, a.natoms,
-                  kMaxServeAtoms);
     spec[s].natoms = a.natoms;
     spec[s].atom_off = a.atom_off;
     for (int d = 0; d < 3; ++d) spec[s].K[d] = a.kmesh[d];
@@ -228,7 +225,7 @@ static int serve_ef_impl(const admp_pools* P, const admp_sys* sys, int nsys, dou
 template <typename T>
 static __global__ void __launch_bounds__(256)
     csr_spmv_finish_kernel(Batch b, QEqParams prm, const long long* __restrict__ pstart, const int* __restrict__ pcnt,
-                           const ColT* __restrict__ col, const T* __restrict__ coef, const T* __restrict__ v,
+                           const int* __restrict__ col, const T* __restrict__ coef, const T* __restrict__ v,
                            T* __restrict__ Hv, const double* __restrict__ diag, const double* __restrict__ zc,
                            CGScal* __restrict__ sc, double* __restrict__ hv_out) {
   __shared__ double red[5 * 32];
@@ -269,7 +266,7 @@ static __global__ void __launch_bounds__(256)
       for (int u = 0; u < kSpmvUnroll; ++u) {
         const int k = k0 + sub + u * kSpmvLanes;
         const bool ok = k < n;
-        c[u] = ok ? d.atom_off + (int)col[st + k] : -1;
+        c[u] = ok ? col[st + k] : -1;
         w[u] = ok ? coef[st + k] : T(0);
       }
       T vv[kSpmvUnroll];

@@ -12,12 +12,6 @@
 
 namespace admp {
 
-// Neighbour columns of the serving CSR rows: the neighbour's index within its
-// system (pool index - atom_off), 16 bits, so a row entry is 2 + sizeof(T)
-// bytes (serving systems hold at most 65535 atoms).
-typedef unsigned short ColT;
-constexpr int kMaxServeAtoms = 65535;
-
 struct SrvSys {          // per-system data of one launch (device array)
   double b[9], bi[9];
   int nc[3];
@@ -253,7 +247,7 @@ static __global__ void __launch_bounds__(256)
     sn_pairs_kernel(Batch b, SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
                     const double4* __restrict__ frac64, const int* __restrict__ cell_of, const int* __restrict__ cells,
                     const int* __restrict__ sorted, int* __restrict__ pcnt, const long long* __restrict__ pstart,
-                    ColT* __restrict__ col) {
+                    int* __restrict__ col) {
   typedef typename Vec4<T>::type V4;
   constexpr int kV4Chunks = sizeof(V4) / 16;
   __shared__ __align__(16) V4 cand[8][2][32];
@@ -414,7 +408,7 @@ static __global__ void __launch_bounds__(256)
               in = rr < rc2 && rr > 1e-4;
             }
             if (in) {
-              if (cnt < row) col[base + cnt] = (ColT)(j - d.atom_off);
+              if (cnt < row) col[base + cnt] = j;
               ++cnt;
             }
           }
@@ -471,7 +465,7 @@ template <typename T>
 static __global__ void __launch_bounds__(256)
     pair_ef_kernel(Batch b, const SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
                    const double4* __restrict__ frac64, const T* __restrict__ q, const T* __restrict__ eta,
-                   const long long* __restrict__ pstart, const int* __restrict__ pcnt, const ColT* __restrict__ col,
+                   const long long* __restrict__ pstart, const int* __restrict__ pcnt, const int* __restrict__ col,
                    double ke, T* __restrict__ grad, double* __restrict__ energy) {
   __shared__ double bx[9];
   __shared__ double red[32];
@@ -503,7 +497,7 @@ static __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int u = 0; u < 3; ++u) {
           const int k = k0 + lane + 32 * u;
-          jj[u] = k < n ? d.atom_off + (int)col[st + k] : -1;
+          jj[u] = k < n ? col[st + k] : -1;
         }
         T drr[3][3], qjj[3], ejj[3];
 #pragma unroll
@@ -572,7 +566,7 @@ template <typename T>
 static __global__ void __launch_bounds__(256)
     csr_coef_kernel(Batch b, const SrvSys* __restrict__ ss, const typename Vec4<T>::type* __restrict__ frac,
                     const T* __restrict__ eta, const long long* __restrict__ pstart, const int* __restrict__ pcnt,
-                    const ColT* __restrict__ col, double ke, T* __restrict__ coef) {
+                    const int* __restrict__ col, double ke, T* __restrict__ coef) {
   __shared__ double bx[9];
   const int s = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc d = b.s[s];
@@ -596,7 +590,7 @@ static __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int u = 0; u < 3; ++u) {
         const int k = k0 + lane + 32 * u;
-        jj[u] = k < n ? d.atom_off + (int)col[st + k] : -1;
+        jj[u] = k < n ? col[st + k] : -1;
       }
       T drr[3][3], ejj[3];
 #pragma unroll

@@ -222,36 +222,12 @@ static int serve_ef_impl(const admp_pools* P, const admp_sys* sys, int nsys, dou
 // qeq_finish_kernel): per row h = (recip + J_real v)_i + diag_i v_i + nn sum(v)
 // (+ slab terms), Hv_i = h, and the block sums of v.h and C.h into the CG
 // scalars -- one pass over the rows instead of two.
-//
-// Each warp takes four rows per round (eight lanes per row).  The rows' column
-// indices and coefficients stream into shared memory by bulk asynchronous
-// copies (TMA engine, one pair of copies per row, completion on the warp's
-// mbarrier), double-buffered: the next round's rows are in flight while the
-// lanes gather v for the current ones.  A row longer than the staging slot
-// reads its entries from global memory directly.
-constexpr int kSpmvRowCap = 128;   // entries staged per row
-constexpr int kSpmvRounds = 4;     // rows per warp and round
-constexpr long long kSpmvSpin = 1LL << 26;  // bounded wait for a round's copies
-
-template <typename T>
-struct SpmvStage {
-  int col[2][kSpmvRounds][kSpmvRowCap];
-  T coef[2][kSpmvRounds][kSpmvRowCap];
-  unsigned long long bar[2];
-};
-
-template <typename T>
-inline size_t spmv_smem() {
-  return 8 * sizeof(SpmvStage<T>);
-}
-
 template <typename T>
 static __global__ void __launch_bounds__(256)
     csr_spmv_finish_kernel(Batch b, QEqParams prm, const long long* __restrict__ pstart, const int* __restrict__ pcnt,
                            const int* __restrict__ col, const T* __restrict__ coef, const T* __restrict__ v,
                            T* __restrict__ Hv, const double* __restrict__ diag, const double* __restrict__ zc,
                            CGScal* __restrict__ sc, double* __restrict__ hv_out) {
-  extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ double red[5 * 32];
   const int s0 = find_sys<F_ATOM>(b, blockIdx.x);
   const SysDesc d = b.s[s0];
@@ -262,105 +238,42 @@ static __global__ void __launch_bounds__(256)
   const bool slab = (prm.flags & ADMP_QEQ_SLAB) != 0;
   const int nc = S.n_const;
   double accs[5] = {0, 0, 0, 0, 0};
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int sub = lane & (kSpmvLanes - 1), grp = lane / kSpmvLanes;  // grp: row of the round
-  SpmvStage<T>& stg = *reinterpret_cast<SpmvStage<T>*>(dsm + warp * sizeof(SpmvStage<T>));
+  const int sub = threadIdx.x & (kSpmvLanes - 1);
+  const int grp = threadIdx.x / kSpmvLanes, ngrp = blockDim.x / kSpmvLanes;
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
-  const int per_round = (blockDim.x >> 5) * kSpmvRounds;
-  // bulk copies need 16-byte aligned rows: the row slots are multiples of 4 entries, so rows qualify when
-  // the arrays and the system's pair region start 16-byte aligned (otherwise every row reads directly)
-  const bool bulk_ok = ((reinterpret_cast<uintptr_t>(col) | reinterpret_cast<uintptr_t>(coef)) & 15) == 0;
-  const int rounds = (a1 - a0 + per_round - 1) / per_round;
-  if (lane == 0) {
-    mbar_init(&stg.bar[0], 1);
-    mbar_init(&stg.bar[1], 1);
-    mbar_init_fence();
+  long long st_next = 0;
+  int n_next = 0;
+  if (a0 + grp < a1) {
+    st_next = pstart[d.atom_off + a0 + grp];
+    n_next = pcnt[d.atom_off + a0 + grp];
   }
-  __syncwarp();
-  // lanes 0 .. kSpmvRounds-1 hold their round's row (start, count) for each buffer
-  long long rst[2] = {0, 0};
-  int rn[2] = {0, 0};
-  // stage round k in buffer bs: lane r < kSpmvRounds issues row r's two copies
-  auto issue = [&](int k, int bs) {
-    const int a = a0 + k * per_round + warp * kSpmvRounds + lane;
-    long long st = 0;
-    int n = 0;
-    if (lane < kSpmvRounds && a < a1) {
-      st = pstart[d.atom_off + a];
-      n = pcnt[d.atom_off + a];
-    }
-    const bool staged = bulk_ok && n > 0 && n <= kSpmvRowCap && (st & 3) == 0;
-    const unsigned ne = staged ? (unsigned)((n + 3) & ~3) : 0u;  // within the row slot (a multiple of 4)
-    unsigned bytes = ne * (unsigned)(sizeof(int) + sizeof(T));
-#pragma unroll
-    for (int o = 1; o < kSpmvRounds; o <<= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
-    if (lane == 0) mbar_arrive_expect_tx(&stg.bar[bs], bytes);
-    __syncwarp();
-    if (staged) {
-      fence_proxy_async_smem();
-      bulk_copy_g2s(stg.col[bs][lane], col + st, ne * (unsigned)sizeof(int), &stg.bar[bs]);
-      bulk_copy_g2s(stg.coef[bs][lane], coef + st, ne * (unsigned)sizeof(T), &stg.bar[bs]);
-    }
-    if (bs) {
-      rst[1] = st;
-      rn[1] = n;
-    } else {
-      rst[0] = st;
-      rn[0] = n;
-    }
-  };
-  unsigned parity[2] = {0u, 0u};
-  if (rounds > 0) issue(0, 0);
-  for (int k = 0; k < rounds; ++k) {
-    const int bs = k & 1;
-    if (k + 1 < rounds) issue(k + 1, bs ^ 1);
-    bool ok = false;
-    for (long long it = 0; it < kSpmvSpin; ++it)
-      if (mbar_try_wait(&stg.bar[bs], parity[bs])) {
-        ok = true;
-        break;
-      }
-    parity[bs] ^= 1u;
-    if (!ok && lane == 0) atomicExch(&sc[s].status, ADMP_ERR_CUDA);
-    const long long st = __shfl_sync(0xffffffffu, bs ? rst[1] : rst[0], grp);
-    const int n = __shfl_sync(0xffffffffu, bs ? rn[1] : rn[0], grp);
-    const int a = a0 + k * per_round + warp * kSpmvRounds + grp;
+  for (int base = a0; base < a1; base += ngrp) {
+    const int a = base + grp;
     const bool row = a < a1;
     const int i = d.atom_off + (row ? a : a0);
+    const long long st = st_next;
+    const int n = row ? n_next : 0;
+    if (a + ngrp < a1) {
+      st_next = pstart[i + ngrp];
+      n_next = pcnt[i + ngrp];
+    }
     T acc = 0;
-    if (bulk_ok && n <= kSpmvRowCap && (st & 3) == 0) {  // the rows issue() staged
-      const int* cs = stg.col[bs][grp];
-      const T* ws = stg.coef[bs][grp];
-      for (int k0 = 0; k0 < n; k0 += kSpmvLanes * kSpmvUnroll) {
-        T vv[kSpmvUnroll], w[kSpmvUnroll];
+    for (int k0 = 0; k0 < n; k0 += kSpmvLanes * kSpmvUnroll) {
+      int c[kSpmvUnroll];
+      T w[kSpmvUnroll];
 #pragma unroll
-        for (int u = 0; u < kSpmvUnroll; ++u) {
-          const int kk = k0 + sub + u * kSpmvLanes;
-          const bool in = kk < n;
-          w[u] = in ? ws[kk] : T(0);
-          vv[u] = in ? v[cs[kk]] : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < kSpmvUnroll; ++u) acc += w[u] * vv[u];
+      for (int u = 0; u < kSpmvUnroll; ++u) {
+        const int k = k0 + sub + u * kSpmvLanes;
+        const bool ok = k < n;
+        c[u] = ok ? col[st + k] : -1;
+        w[u] = ok ? coef[st + k] : T(0);
       }
-    } else {
-      for (int k0 = 0; k0 < n; k0 += kSpmvLanes * kSpmvUnroll) {
-        int c[kSpmvUnroll];
-        T w[kSpmvUnroll];
+      T vv[kSpmvUnroll];
 #pragma unroll
-        for (int u = 0; u < kSpmvUnroll; ++u) {
-          const int kk = k0 + sub + u * kSpmvLanes;
-          const bool in = kk < n;
-          c[u] = in ? col[st + kk] : -1;
-          w[u] = in ? coef[st + kk] : T(0);
-        }
-        T vv[kSpmvUnroll];
+      for (int u = 0; u < kSpmvUnroll; ++u) vv[u] = c[u] >= 0 ? v[c[u]] : T(0);
 #pragma unroll
-        for (int u = 0; u < kSpmvUnroll; ++u) vv[u] = c[u] >= 0 ? v[c[u]] : T(0);
-#pragma unroll
-        for (int u = 0; u < kSpmvUnroll; ++u) acc += w[u] * vv[u];
-      }
+      for (int u = 0; u < kSpmvUnroll; ++u) acc += w[u] * vv[u];
     }
 #pragma unroll
     for (int o = kSpmvLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -379,7 +292,6 @@ static __global__ void __launch_bounds__(256)
       for (int cc = 0; cc < kMaxConst; ++cc)  // serving constraints are total-charge rows
         if (cc < nc) accs[1 + cc] += h;
     }
-    __syncwarp();  // buffer bs is refilled by the next round's issue
   }
   double a1v[1] = {accs[0]};
   block_atomic_sum<1>(a1v, &sc[s].pHp, red);
@@ -398,9 +310,7 @@ static int srv_matvec(const admp_pools* P, const RecipPlan<T>& plan, QEqParams p
                                     P->acc, ke, Hv, st, P->sorted, (const T*)P->green);
   if (s) return s;
   int h = prof_begin(st);
-  ADMP_CUDA_TRY(ensure_smem(csr_spmv_finish_kernel<T>, spmv_smem<T>()));
-  csr_spmv_finish_kernel<T><<<b.nblk_atom, 256, spmv_smem<T>(), st>>>(b, prm, P->pstart, P->pcnt, P->col,
-                                                                   (const T*)P->coef, v,
+  csr_spmv_finish_kernel<T><<<b.nblk_atom, 256, 0, st>>>(b, prm, P->pstart, P->pcnt, P->col, (const T*)P->coef, v,
                                                          Hv, P->cg_diag, P->cg_z, (CGScal*)P->cg_state, hv_out);
   prof_end(h, PK_CSR_SPMV, -1.0, st);
   count_launches(1);

@@ -24,13 +24,6 @@ struct SrvSys {          // per-system data of one launch (device array)
   int slot;
 };
 
-// Row slot of each atom in its system's pair region: pair_cap / natoms rounded
-// down to a multiple of 4 entries, so every row starts 16-byte aligned (the
-// pair regions are 64-entry aligned) for the bulk copies of the SpMV.
-__device__ __forceinline__ long long row_slot(long long pair_cap, int natoms) {
-  return (pair_cap / (natoms > 0 ? natoms : 1)) & ~3LL;
-}
-
 template <typename T>
 struct Vec4 {
   typedef float4 type;
@@ -108,7 +101,7 @@ static __global__ void __launch_bounds__(256)
   const SrvSys& S = ss[s];
   const int a0 = (blockIdx.x - d.blk_atom) * b.apb;
   const int a1 = min(a0 + b.apb, d.natoms);
-  const long long row = row_slot(S.pair_cap, d.natoms);  // fixed row slot per atom
+  const long long row = S.pair_cap / (d.natoms > 0 ? d.natoms : 1);  // fixed row slot per atom
   for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     const int i = d.atom_off + a;
     pcnt[i] = 0;
@@ -199,39 +192,6 @@ __device__ __forceinline__ void sn_offsets(int nc, int* off, int& n) {
   }
 }
 
-// One-dimensional bulk asynchronous copies global -> shared through the TMA
-// engine (cp.async.bulk, no tensor map and no multicast): both addresses
-// 16-byte aligned, the size a multiple of 16 bytes, completion counted in
-// bytes on a shared-memory mbarrier.
-__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
-  asm volatile(
-      "{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(smem_addr(bar)),
-      "r"(bytes)
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// order this thread's earlier generic-proxy accesses of shared memory before its later bulk copies
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-
 // Asynchronous 16-byte global -> shared copies (cp.async, sm_80+): the
 // issuing warp does not wait for them until cp.async.wait_group.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -274,7 +234,7 @@ __device__ __forceinline__ SnChunk sn_next(SnChunk c, const int* tb_begin, const
 // loads per candidate.  Rows keep the order of a per-atom scan: neighbour
 // cells in (x, y, z) offset order, candidates in sorted order.  One pass:
 // each atom writes its neighbours into its fixed row slot col[pstart[i] ..]
-// (pstart from sn_bin_kernel, row = row_slot(pair_cap, natoms)) and pcnt[i]; a row
+// (pstart from sn_bin_kernel, row = pair_cap / natoms) and pcnt[i]; a row
 // that would overflow its slot keeps the first `row` entries, sets the
 // system's status to ADMP_ERR_CAPACITY and raises pair_need to natoms x
 // (longest row).  Unbinned atoms keep pcnt = 0.
@@ -298,7 +258,7 @@ static __global__ void __launch_bounds__(256)
   SrvSys& S = ss[s];
   if (S.status) return;  // sn_bin_kernel left every count of a failed system at zero
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const long long row = row_slot(S.pair_cap, d.natoms);
+  const long long row = S.pair_cap / (d.natoms > 0 ? d.natoms : 1);
   const int n = S.ncells;
   const int* start = cells + S.cell_off + (n + 1);
   const double rc2 = S.rc * S.rc;
@@ -463,7 +423,7 @@ static __global__ void __launch_bounds__(256)
         pcnt[i] = cnt < row ? cnt : (int)row;
         if (cnt > row) {
           S.status = ADMP_ERR_CAPACITY;  // every writer stores the same value
-          atomicMax(&S.pair_need, (long long)d.natoms * ((cnt + 3) & ~3));
+          atomicMax(&S.pair_need, (long long)d.natoms * cnt);
         }
       }
     }

@@ -415,12 +415,4 @@ __device__ Cplx<T>* fft_lines(Cplx<T>* a, Cplx<T>* b, int nl, int n, int ls, int
   return fft_run<T, LINE_FAST, false, INV, NL>(R, a, b, nl, n, ls, es, W, threadIdx.x, blockDim.x);
 }
 
-// One contiguous line of length n transformed by one warp (lane = 0..31),
-// ping-ponging between a and b; the caller __syncwarp()s after writing a.
-template <typename T, bool INV>
-__device__ __forceinline__ Cplx<T>* warp_fft(const Radices& R, Cplx<T>* a, Cplx<T>* b, int n, const Cplx<T>* W,
-                                             int lane) {
-  return fft_run<T, false, true, INV>(R, a, b, 1, n, n, 1, W, lane, 32);
-}
-
 }  // namespace admp

@@ -57,7 +57,7 @@ __device__ __forceinline__ int fdiv(int x, const FastDiv& f) {
 // compile time, so the split is a mask and a shift.
 template <bool LINE_FAST, int NL>
 __device__ __forceinline__ void split_item(int idx, const FastDiv& f, int& l, int& j) {
-  if (LINE_FAST && NL > 0) {
+  if constexpr (LINE_FAST && NL > 0) {
     l = idx & (NL - 1);
     j = idx / NL;
   } else {

@@ -3,6 +3,7 @@
 
 #include <vector>
 
+#include "dft_tc.cuh"
 #include "pme_kernels.cuh"
 #include "runtime.h"
 
@@ -30,6 +31,8 @@ struct RecipPlan {
   bool slab = false;
   int buf_elems = 0;
   size_t smem_slab = 0;
+  // FP32 CG matvecs: x pass on the tensor cores (every K0 <= kTcMaxK)
+  bool tc_x = false;
 };
 
 // The per-system table as one by-value parameter: the only launch of a call
@@ -65,7 +68,12 @@ inline Batch family_batch(const RecipPlan<T>& p, int F) {
   b.fam = F;
   for (int s = 0; s < b.nsys; ++s) {
     const SysDesc& d = p.hs[s];
-    b.blk[s] = F == F_ATOM ? d.blk_atom : F == F_Z ? d.blk_z : F == F_Y ? d.blk_y : F == F_X ? d.blk_x : d.blk_slab;
+    b.blk[s] = F == F_ATOM ? d.blk_atom
+               : F == F_Z  ? d.blk_z
+               : F == F_Y  ? d.blk_y
+               : F == F_X  ? d.blk_x
+               : F == F_XT ? d.blk_xt
+                           : d.blk_slab;
   }
   return b;
 }
@@ -81,6 +89,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   b.apb = 256;
   b.done = nullptr;
   b.done_stride = 0;
+  b.status_off = 0;
   b.s = nullptr;
   int maxK[3] = {1, 1, 1};
   for (int s = 0; s < nsys; ++s)
@@ -108,7 +117,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   p.smem_x = (2 * (size_t)zb + 1) * maxK[0] * cs + ((size_t)maxK[0] + 2 * zb) * 8 + (size_t)zb * 16;
   if (p.smem_z > 227 * 1024 || p.smem_y > 227 * 1024 || p.smem_x > 227 * 1024)
     return fail(ADMP_ERR_MESH, "mesh %dx%dx%d too large for the shared-memory FFT", maxK[0], maxK[1], maxK[2]);
-  int ba = 0, bz = 0, by = 0, bx = 0;
+  int ba = 0, bz = 0, by = 0, bx = 0, bxt = 0;
   size_t mo = 0, so = 0;
   for (int s = 0; s < nsys; ++s) {
     SysDesc& d = p.hs[s];
@@ -125,6 +134,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
     d.blk_z = bz;
     d.blk_y = by;
     d.blk_x = bx;
+    d.blk_xt = bxt;
     d.mesh_off = (int64_t)mo;
     d.spec_off = (int64_t)so;
     d.green_off = sys[s].green_off >= 0 ? (int64_t)sys[s].green_off : (int64_t)so;
@@ -133,10 +143,13 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
     bz += ((d.K0 * d.K1 + 1) / 2 + lp - 1) / lp;
     by += d.K0 * ncb;
     bx += (d.K1 * d.K2h + zb - 1) / zb;  // x passes: runs of zb flattened (y, kz) columns
+    bxt += (d.K1 * d.K2h + kTcRows - 1) / kTcRows;
     mo += align_up((size_t)d.K0 * d.K1 * d.K2, 64);
     so += align_up((size_t)d.K0 * d.K1 * d.K2h, 32);
   }
   b.nblk_atom = ba;
+  b.nblk_xt = bxt;
+  p.tc_x = sizeof(T) == 4 && maxK[0] <= kTcMaxK;
   b.nblk_z = bz;
   b.nblk_y = by;
   b.nblk_x = bx;
@@ -203,9 +216,14 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
     if (b.nblk_y) fft_y_kernel<T, false><<<b.nblk_y, 256, p.smem_y, st>>>(by, spec);
     prof_end(h, PK_FFT_Y_FWD, 2 * cb, st);
   }
+  const uint32_t* tct = (green && p.tc_x) ? tc_tables(st) : nullptr;
+  if (tct) ADMP_CUDA_TRY(ensure_smem(tc_x_apply_kernel, (size_t)kTcSmem));
   h = prof_begin(st);
   if (b.nblk_x) {
-    if (green)
+    if (tct)
+      tc_x_apply_kernel<<<b.nblk_xt, 256, kTcSmem, st>>>(family_batch(p, F_XT), (Cplx<float>*)spec,
+                                                          (const float*)green, tct);
+    else if (green)
       fft_x_apply_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(bx, spec, green);
     else
       fft_x_green_kernel<T><<<b.nblk_x, 256, p.smem_x, st>>>(bx, spec, box, acc, ke);

@@ -22,6 +22,7 @@ struct SysDesc {
   int32_t atom_off, natoms;
   int32_t K0, K1, K2, K2h;
   int32_t blk_atom, blk_z, blk_y, blk_x, blk_slab;
+  int32_t blk_xt;  // first block of the tensor-core x pass (128 columns per block)
   int64_t mesh_off, spec_off;
   int64_t green_off;  // cached 2 G_s (half-spectrum layout) for CG matvecs
   double kappa;
@@ -35,13 +36,14 @@ struct SysDesc {
 // of a call do not each carry the whole table as a kernel parameter).
 struct Batch {
   int nsys;
-  int nblk_atom, nblk_z, nblk_y, nblk_x, nblk_slab;
+  int nblk_atom, nblk_z, nblk_y, nblk_x, nblk_slab, nblk_xt;
   int apb;  // atoms per block (atom kernels)
   int lp;   // line pairs per block (z passes)
   int zb;   // columns per block (y / x passes)
   int maxK0, maxK1, maxK2;
   const int* done;   // optional per-slot skip flags (done[slot * done_stride], slot = box_idx)
   int done_stride;
+  int status_off;    // ints from a slot's done flag to its status word (errors of bounded waits)
   const SysDesc* s;  // device table [nsys]
   // first block of every system in the block family `fam` of this launch (a
   // copy of the table's blk_* column, ~1 KB): a block finds its system by
@@ -62,11 +64,16 @@ constexpr int kAccVk = 1;       // 9: dE/dB (B = box^-1) through k vectors
 constexpr int kAccWf = 10;      // 9: dE/dB through fractional coordinates
 constexpr int kAccSlots = 19;
 
-enum SysField { F_ATOM = 0, F_Z = 1, F_Y = 2, F_X = 3, F_SLAB = 4 };
+enum SysField { F_ATOM = 0, F_Z = 1, F_Y = 2, F_X = 3, F_SLAB = 4, F_XT = 5 };
 
 template <int F>
 __device__ __forceinline__ int blk_of(const SysDesc& d) {
-  return F == F_ATOM ? d.blk_atom : F == F_Z ? d.blk_z : F == F_Y ? d.blk_y : F == F_X ? d.blk_x : d.blk_slab;
+  return F == F_ATOM ? d.blk_atom
+         : F == F_Z  ? d.blk_z
+         : F == F_Y  ? d.blk_y
+         : F == F_X  ? d.blk_x
+         : F == F_XT ? d.blk_xt
+                     : d.blk_slab;
 }
 
 template <int F>

@@ -182,6 +182,7 @@ static int qeq_solve_impl(int flags, int nf, int N, const int* kmesh, const T* p
   RecipPlan<T> pl = c.w.plan;
   pl.b.done = &c.w.sc->done;
   pl.b.done_stride = (int)(sizeof(CGScal) / sizeof(int));
+  pl.b.status_off = (int)((offsetof(CGScal, status) - offsetof(CGScal, done)) / sizeof(int));
   c.w.plan = pl;
   const int chunk = 8;
   int it = 0;

@@ -388,6 +388,7 @@ static int serve_qeq_iterate_impl(const admp_pools* P, const admp_sys* sys, int 
   CGScal* sc = (CGScal*)P->cg_state;
   plan.b.done = &sc[0].done;
   plan.b.done_stride = (int)(sizeof(CGScal) / sizeof(int));
+  plan.b.status_off = (int)((offsetof(CGScal, status) - offsetof(CGScal, done)) / sizeof(int));
   const Batch& b = plan.b;
   const QEqParams prm = srv_params(tol, max_iter, ke);
   for (int k = 0; k < niter; ++k) {

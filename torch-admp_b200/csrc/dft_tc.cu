@@ -7,7 +7,7 @@
 
 namespace admp {
 
-static __device__ __align__(128) uint32_t g_tc_tab[kTcMaxK + 1][4][kTcImgWords];
+static __device__ __align__(128) uint32_t g_tc_tab[kTcMaxK + 1][4][2][kTcImgWords];
 
 // Phi[x][j']: cos(2 pi x j' / K0) for j' <= K0 / 2 (j' < 40); sin(2 pi x (j' - 40) / K0) for
 // 1 <= j' - 40 <= (K0 - 1) / 2; zero elsewhere and for x >= K0.  Arguments reduced exactly mod K0.
@@ -25,18 +25,18 @@ __device__ double tc_phi(int K0, int x, int j) {
   return s;
 }
 
+// Part 0 / 1: rows j' (0..79), columns x - 40 part (stage 1); part 2 / 3: rows x (0..79), columns
+// j' - 40 (part - 2) (stage 3).  Head and tail images of each.
 static __global__ void tc_table_kernel() {
   const int K0 = blockIdx.x + 1;
-  for (int e = threadIdx.x; e < kTcCols * kTcCols; e += blockDim.x) {
-    const int r = e / kTcCols, k = e % kTcCols;
+  for (int e = threadIdx.x; e < 4 * kTcN * kTcHalf; e += blockDim.x) {
+    const int part = e / (kTcN * kTcHalf), rem = e % (kTcN * kTcHalf);
+    const int r = rem / kTcHalf, k = rem % kTcHalf;
+    const float p = part < 2 ? (float)tc_phi(K0, k + kTcHalf * part, r) : (float)tc_phi(K0, r, k + kTcHalf * (part - 2));
     const int w = tc_off(r, k) >> 2;
-    // stage 1: row r = j', column k = x;  stage 3: row r = x, column k = j'
-    const float p1 = (float)tc_phi(K0, k, r), p3 = (float)tc_phi(K0, r, k);
-    const uint32_t h1 = tf32_head(p1), h3 = tf32_head(p3);
-    g_tc_tab[K0][0][w] = h1;
-    g_tc_tab[K0][1][w] = tf32_head(p1 - __uint_as_float(h1));
-    g_tc_tab[K0][2][w] = h3;
-    g_tc_tab[K0][3][w] = tf32_head(p3 - __uint_as_float(h3));
+    const uint32_t h = tf32_head(p);
+    g_tc_tab[K0][part][0][w] = h;
+    g_tc_tab[K0][part][1][w] = tf32_head(p - __uint_as_float(h));
   }
 }
 

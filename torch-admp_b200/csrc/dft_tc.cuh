@@ -23,15 +23,19 @@
 //
 // Layout.  Operands are K-major without swizzle: an 8-row x 16-byte core
 // matrix per (row group, 4 columns), 128 bytes apart along K (LBO) and
-// kTcSbo bytes apart along M/N (SBO).  Each tile is 80 columns (K) wide.
-// Per CTA: A = 4 tiles of 128 x 80 (re / im, head / tail), B = 2 tiles of
-// 80 x 80 (head / tail), 210 KB of shared memory; TMEM: 256 columns (the
-// real accumulator at column 0, the imaginary one at column 128).  The two
-// B images per mesh length (Phi^T for stage 1, Phi for stage 3, head and
-// tail) are built once per device in global memory and copied into shared
-// memory by 1-D bulk asynchronous copies (the TMA engine, no tensor map,
-// no multicast) on an mbarrier.  Every wait is bounded; on expiry the
-// system's CG status is set and the kernel returns after freeing its TMEM.
+// kTcSbo bytes apart along M/N (SBO).  The contraction of each stage runs
+// in two halves of 40 columns (x < 40 and x >= 40 in stage 1; the U and the
+// V columns in stage 3), so a CTA holds only one half: A = 4 tiles of
+// 128 x 40 (re / im, head / tail) and B = 2 tiles of 80 x 40 (head / tail),
+// 105 KB of shared memory, and two CTAs share an SM, one CTA's loads and
+// Green's-function step overlapping the other's products.  TMEM: 256
+// columns per CTA (the real accumulator at column 0, the imaginary one at
+// column 128).  The B halves (Phi^T for stage 1, Phi for stage 3, head and
+// tail) of every mesh length are built once per device in global memory
+// and copied into shared memory by 1-D bulk asynchronous copies (the TMA
+// engine, no tensor map, no multicast) on an mbarrier.  Every wait is
+// bounded; on expiry the system's CG status is set and the kernel returns
+// after freeing its TMEM.
 #pragma once
 
 #include <cstddef>
@@ -41,17 +45,18 @@
 
 namespace admp {
 
-constexpr int kTcMaxK = 79;               // longest x line of this path (40 cos + 40 sin columns)
-constexpr int kTcRows = 128;              // flattened columns per CTA (MMA M)
-constexpr int kTcCols = 80;               // K width of every operand tile, N of stage 1
-constexpr int kTcSbo = (kTcCols / 4) * 128;
-constexpr int kTcATile = kTcRows * kTcCols * 4;  // bytes
-constexpr int kTcBTile = kTcCols * kTcCols * 4;
+constexpr int kTcMaxK = 79;                       // longest x line of this path (40 cos + 40 sin columns)
+constexpr int kTcRows = 128;                      // flattened columns per CTA (MMA M)
+constexpr int kTcN = 80;                          // N of stage 1 (40 cos + 40 sin columns)
+constexpr int kTcHalf = 40;                       // K columns of one half of a contraction
+constexpr int kTcSbo = (kTcHalf / 4) * 128;       // bytes between 8-row groups
+constexpr int kTcATile = kTcRows * kTcHalf * 4;   // bytes
+constexpr int kTcBTile = kTcN * kTcHalf * 4;
 constexpr int kTcSmem = 4 * kTcATile + 2 * kTcBTile;
-constexpr int kTcImgWords = kTcCols * kTcCols;   // one B image
+constexpr int kTcImgWords = kTcN * kTcHalf;       // one B image (one half, head or tail)
 constexpr long long kTcSpin = 1LL << 24;
 
-// byte offset of (row r, column k) in a K-major no-swizzle tile
+// byte offset of (row r, column k) in a K-major no-swizzle tile kTcHalf columns wide
 __host__ __device__ __forceinline__ int tc_off(int r, int k) {
   return (r >> 3) * kTcSbo + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4;
 }
@@ -98,7 +103,7 @@ __device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// the two B images (head, tail) of one stage: 2 x 25,600 bytes by the bulk-copy engine
+// one B half (head and tail images, 2 x 12,800 bytes) by the bulk-copy engine
 __device__ __forceinline__ void tc_load_b(unsigned char* dst, const uint32_t* src, uint64_t* bar) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem(bar)), "r"(2 * kTcBTile)
                : "memory");
@@ -108,6 +113,28 @@ __device__ __forceinline__ void tc_load_b(unsigned char* dst, const uint32_t* sr
             tc_smem(dst + h * kTcBTile)),
         "l"(src + (size_t)h * kTcImgWords), "r"(kTcBTile), "r"(tc_smem(bar))
         : "memory");
+}
+
+// The three-term products of one contraction half, issued by one thread: D_re += A_re B,
+// D_im += A_im B over ks K-steps (8 columns each, 256 bytes apart in every tile, i.e. 16 in the
+// descriptors' start-address field).  `acc`: accumulate onto the earlier half.
+__device__ __forceinline__ void tc_products(uint32_t dre, uint32_t dim, const unsigned char* Arh,
+                                            const unsigned char* Arl, const unsigned char* Aih,
+                                            const unsigned char* Ail, const unsigned char* Bt, int ks, int n,
+                                            bool acc) {
+  const uint32_t id = tc_idesc(n);
+  const uint64_t arh = tc_desc(tc_smem(Arh)), arl = tc_desc(tc_smem(Arl)), aih = tc_desc(tc_smem(Aih)),
+                 ail = tc_desc(tc_smem(Ail)), bh = tc_desc(tc_smem(Bt)), bl = tc_desc(tc_smem(Bt + kTcBTile));
+  for (int k = 0; k < ks; ++k) {
+    const uint64_t o = (uint64_t)k * 16;
+    const uint32_t first = (acc || k > 0) ? 1u : 0u;
+    tc_mma(dre, arh + o, bh + o, id, first);  // head * head
+    tc_mma(dim, aih + o, bh + o, id, first);
+    tc_mma(dre, arh + o, bl + o, id, 1u);     // head * tail
+    tc_mma(dim, aih + o, bl + o, id, 1u);
+    tc_mma(dre, arl + o, bh + o, id, 1u);     // tail * head
+    tc_mma(dim, ail + o, bh + o, id, 1u);
+  }
 }
 
 #define ADMP_TC_LD4(taddr, v)                                                                           \
@@ -135,10 +162,10 @@ __device__ __forceinline__ void tc_put4(unsigned char* hi, unsigned char* lo, in
   *reinterpret_cast<uint4*>(lo + o) = l;
 }
 
-// The B images of every mesh length 1..kTcMaxK, [K0][stage 1 head, stage 1
-// tail, stage 3 head, stage 3 tail][kTcImgWords] (dft_tc.cu): built on the
-// current device at the first call (ordered on `st` and waited for, so any
-// stream may read them afterwards).  nullptr if they cannot be built.
+// The B images of every mesh length 1..kTcMaxK, [K0][part][head, tail][kTcImgWords] with parts
+// 0, 1 = stage 1 (Phi^T restricted to x < 40, x >= 40) and 2, 3 = stage 3 (Phi restricted to
+// j' < 40, j' >= 40) (dft_tc.cu): built on the current device at the first call (ordered on `st`
+// and waited for, so any stream may read them afterwards).  nullptr if they cannot be built.
 const uint32_t* tc_tables(cudaStream_t st);
 
 // One tile: 128 flattened columns of one system (block family F_XT).
@@ -163,7 +190,8 @@ __device__ __forceinline__ bool tc_tile(const Batch& b, int t, TcTile& T) {
   return true;
 }
 
-// A thread's part of a tile's spectrum: column tid % 128, x runs (tid / 128) * 4 + 8 m (m < 10)
+// A thread's part of a tile's spectrum: column tid % 128, x runs (tid / 128) * 4 + 8 m (m < 10);
+// runs m < 5 lie in the first contraction half (x < 40), m >= 5 in the second.
 __device__ __forceinline__ void tc_fetch(const Cplx<float>* __restrict__ spec, const TcTile& T, int tid,
                                          Cplx<float> (&v)[10][4]) {
   const Cplx<float>* H = spec + T.spec_off + T.c0;
@@ -180,26 +208,27 @@ __device__ __forceinline__ void tc_fetch(const Cplx<float>* __restrict__ spec, c
     }
 }
 
+// runs M0 .. M0+4 of the thread's values into the A tiles (columns x - 40 * (M0 / 5))
+template <int M0>
 __device__ __forceinline__ void tc_stage_a(unsigned char* Arh, unsigned char* Arl, unsigned char* Aih,
                                            unsigned char* Ail, int tid, const Cplx<float> (&v)[10][4]) {
   const int ca = tid & (kTcRows - 1), xa = (tid >> 7) * 4;
 #pragma unroll
-  for (int m = 0; m < 10; ++m) {
+  for (int mm = 0; mm < 5; ++mm) {
+    const int m = M0 + mm;
     float re[4], im[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       re[t] = v[m][t].x;
       im[t] = v[m][t].y;
     }
-    tc_put4(Arh, Arl, ca, xa + 8 * m, re);
-    tc_put4(Aih, Ail, ca, xa + 8 * m, im);
+    tc_put4(Arh, Arl, ca, xa + 8 * mm, re);
+    tc_put4(Aih, Ail, ca, xa + 8 * mm, im);
   }
 }
 
-// One CTA per tile (210 KB of shared memory: one CTA per SM), 256 threads.  (A grid of one CTA per
-// SM walking its tiles, loading the next tile's spectrum into registers during the current tile's
-// products, measured 5% slower: static tile assignment over systems of unequal mesh length.)
-static __global__ void __launch_bounds__(256, 1)
+// Two CTAs per SM (105 KB of shared memory each), one tile per CTA, 256 threads.
+static __global__ void __launch_bounds__(256, 2)
     tc_x_apply_kernel(Batch b, Cplx<float>* __restrict__ spec, const float* __restrict__ green,
                       const uint32_t* __restrict__ tab) {
   extern __shared__ __align__(1024) unsigned char tsm[];
@@ -213,25 +242,23 @@ static __global__ void __launch_bounds__(256, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   TcTile cur;
   if (!tc_tile(b, blockIdx.x, cur)) return;
-  const int K0 = cur.K0;
+  const int K0 = cur.K0, h0 = K0 / 2, ns = (K0 - 1) / 2;
   const size_t xs = cur.xs;
-  const uint32_t* tb = tab + (size_t)K0 * 4 * kTcImgWords;
+  const uint32_t* tb = tab + (size_t)K0 * 8 * kTcImgWords;  // [part][head, tail]
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar_b)));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar_m)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    tc_load_b(Bt, tb, &bar_b);  // stage 1 images
+    tc_load_b(Bt, tb, &bar_b);  // stage 1, x < 40
   }
   __syncwarp();
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(tc_smem(&tslot)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  {
-    Cplx<float> v[10][4];
-    tc_fetch(spec, cur, tid, v);  // all 40 loads of a thread in flight before the first use
-    tc_stage_a(Arh, Arl, Aih, Ail, tid, v);
-  }
+  Cplx<float> v[10][4];
+  tc_fetch(spec, cur, tid, v);  // all 40 loads of a thread in flight before the first use
+  tc_stage_a<0>(Arh, Arl, Aih, Ail, tid, v);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -240,144 +267,161 @@ static __global__ void __launch_bounds__(256, 1)
   const uint32_t dre = tm, dim = tm + 128;
   const int q = warp & 3, half = warp >> 2, row = q * 32 + lane;
   const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+  const int c = cur.c0 + row;
+  const bool live = row < cur.nz;
+  uint32_t pb = 0, pm = 0;  // completed phases of bar_b and bar_m
   bool ok = true;
-  {
-    // stage 1: D_re = A_re Phi, D_im = A_im Phi over ceil(K0 / 8) K-steps
-    if (tid == 0) {
-      ok = tc_wait(&bar_b, 0);
+  // one contraction half: B copy awaited, products issued and committed by thread 0, then every
+  // thread waits for them; the verdict is block-uniform
+  auto run_half = [&](int ks, int n, bool acc) {
+    if (tid == 0 && ok) {
+      ok = tc_wait(&bar_b, pb & 1);
       if (ok) {
-        const uint32_t id = tc_idesc(kTcCols);
-        const uint32_t a_r[2] = {tc_smem(Arh), tc_smem(Arl)}, a_i[2] = {tc_smem(Aih), tc_smem(Ail)};
-        const uint32_t bb[2] = {tc_smem(Bt), tc_smem(Bt + kTcBTile)};
-        const int ks = (K0 + 7) >> 3;
-        for (int k = 0; k < ks; ++k)
-          for (int u = 0; u < 3; ++u) {  // head*head, head*tail, tail*head
-            const int ia = u == 2 ? 1 : 0, ib = u == 1 ? 1 : 0;
-            const uint32_t acc = (k > 0 || u > 0) ? 1u : 0u;
-            tc_mma(dre, tc_desc(a_r[ia] + k * 256), tc_desc(bb[ib] + k * 256), id, acc);
-            tc_mma(dim, tc_desc(a_i[ia] + k * 256), tc_desc(bb[ib] + k * 256), id, acc);
-          }
+        tc_products(dre, dim, Arh, Arl, Aih, Ail, Bt, ks, n, acc);
         tc_commit(&bar_m);
       }
     }
-    // the Green's function of this thread's row and k' range, loaded while the products run
-    const int c = cur.c0 + row;
-    const bool live = row < cur.nz;
-    float g1[20], g2[20];
-    {
-      const float* G = green + cur.green_off + c;
-#pragma unroll
-      for (int u = 0; u < 20; ++u) {
-        const int k = half * 20 + u;
-        const bool in = live && k <= K0 / 2;
-        g1[u] = in ? G[(size_t)k * xs] : 0.f;
-        g2[u] = in ? G[(size_t)((K0 - k) % K0) * xs] : 0.f;
-      }
-    }
-    ok = __syncthreads_and(ok) != 0;  // thread 0's verdict (the others hold true)
-    ok = __syncthreads_and(ok && tc_wait(&bar_m, 0)) != 0;
+    ++pb;
+  };
+  auto await_half = [&]() {
+    ok = __syncthreads_and(ok) != 0;
+    ok = __syncthreads_and(ok && tc_wait(&bar_m, pm & 1)) != 0;
+    ++pm;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // the B region is free once stage 1 has completed: stage 3 images
-    if (tid == 0 && ok) tc_load_b(Bt, tb + 2 * (size_t)kTcImgWords, &bar_b);
-    if (ok) {
-      // epilogue 1: k' in [20 half, 20 half + 20), four at a time
-#pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        const int k0 = half * 20 + 4 * i;
-        if (k0 > K0 / 2) break;  // block-uniform
-        uint32_t ea[4], oa[4], eb[4], ob[4];
-        ADMP_TC_LD4(dre + lane_base + k0, ea);
-        ADMP_TC_LD4(dre + lane_base + 40 + k0, oa);
-        ADMP_TC_LD4(dim + lane_base + k0, eb);
-        ADMP_TC_LD4(dim + lane_base + 40 + k0, ob);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        float ur[4], ui[4], vr[4], nvi[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int k = k0 + u;
-          const float Ea = __uint_as_float(ea[u]), Oa = __uint_as_float(oa[u]);
-          const float Eb = __uint_as_float(eb[u]), Ob = __uint_as_float(ob[u]);
-          const float ga = g1[4 * i + u], gb = g2[4 * i + u];
-          if (k == 0 || 2 * k == K0) {  // stands alone: S = (Ea, Eb)
-            ur[u] = ga * Ea;
-            ui[u] = ga * Eb;
-            vr[u] = 0.f;
-            nvi[u] = 0.f;
-          } else {  // zero past K0 / 2 through g
-            const float t1r = ga * (Ea + Ob), t1i = ga * (Eb - Oa);
-            const float t2r = gb * (Ea - Ob), t2i = gb * (Eb + Oa);
-            ur[u] = t1r + t2r;
-            ui[u] = t1i + t2i;
-            vr[u] = t1r - t2r;
-            nvi[u] = t2i - t1i;
-          }
-        }
-        tc_put4(Arh, Arl, row, k0, ur);
-        tc_put4(Arh, Arl, row, 40 + k0, nvi);
-        tc_put4(Aih, Ail, row, k0, ui);
-        tc_put4(Aih, Ail, row, 40 + k0, vr);
-      }
-    }
-    // columns the loop above did not reach still hold stage 1 inputs: zero them (their B rows are
-    // zero too, but stale tails could hold non-finite bit patterns)
-    for (int it = tid; it < kTcRows * 20; it += 256) {
-      const int r = it & (kTcRows - 1), k4 = (it >> 7) * 4;  // k4 in [0, 80)
-      const int kk = k4 < 40 ? k4 : k4 - 40;
-      if (ok && kk <= K0 / 2) continue;
-      const float z[4] = {0.f, 0.f, 0.f, 0.f};
-      tc_put4(Arh, Arl, r, k4, z);
-      tc_put4(Aih, Ail, r, k4, z);
-    }
+  };
+  auto publish = [&]() {  // generic-proxy shared-memory writes -> the products
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // stage 3: out_re = A3_re Phi^T, out_im = A3_im Phi^T (N = x rows, 16-aligned past K0)
-    if (tid == 0 && ok) {
-      ok = tc_wait(&bar_b, 1);
-      if (ok) {
-        const uint32_t id = tc_idesc(((K0 + 15) >> 4) << 4);
-        const uint32_t a_r[2] = {tc_smem(Arh), tc_smem(Arl)}, a_i[2] = {tc_smem(Aih), tc_smem(Ail)};
-        const uint32_t bb[2] = {tc_smem(Bt), tc_smem(Bt + kTcBTile)};
-        for (int k = 0; k < kTcCols / 8; ++k)
-          for (int u = 0; u < 3; ++u) {
-            const int ia = u == 2 ? 1 : 0, ib = u == 1 ? 1 : 0;
-            const uint32_t acc = (k > 0 || u > 0) ? 1u : 0u;
-            tc_mma(dre, tc_desc(a_r[ia] + k * 256), tc_desc(bb[ib] + k * 256), id, acc);
-            tc_mma(dim, tc_desc(a_i[ia] + k * 256), tc_desc(bb[ib] + k * 256), id, acc);
-          }
-        tc_commit(&bar_m);
-      }
+  };
+  // stage 1: D = A Phi over x < 40, then x >= 40
+  run_half(min(5, (K0 + 7) >> 3), kTcN, false);
+  await_half();
+  if (K0 > kTcHalf) {
+    if (tid == 0 && ok) tc_load_b(Bt, tb + 2 * (size_t)kTcImgWords, &bar_b);  // stage 1, x >= 40
+    tc_stage_a<5>(Arh, Arl, Aih, Ail, tid, v);
+    publish();
+    run_half((K0 - kTcHalf + 7) >> 3, kTcN, true);
+  }
+  // the Green's function of this thread's row and k' range, loaded while the products run
+  float g1[20], g2[20];
+  {
+    const float* G = green + cur.green_off + c;
+#pragma unroll
+    for (int u = 0; u < 20; ++u) {
+      const int k = half * 20 + u;
+      const bool in = live && k <= h0;
+      g1[u] = in ? G[(size_t)k * xs] : 0.f;
+      g2[u] = in ? G[(size_t)((K0 - k) % K0) * xs] : 0.f;
     }
-    ok = __syncthreads_and(ok) != 0;
-    ok = __syncthreads_and(ok && tc_wait(&bar_m, 1)) != 0;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (K0 > kTcHalf) await_half();
+  // stage 3 inputs: U (cos columns) into the A tiles now, V (sin columns) kept for the second half
+  if (tid == 0 && ok) tc_load_b(Bt, tb + 4 * (size_t)kTcImgWords, &bar_b);  // stage 3, j' < 40
+  const int nch = h0 >= half * 20 ? min(5, (h0 - half * 20) / 4 + 1) : 0;  // block-uniform
+  float wr[20], wi[20];  // V_re, -V_im of k' = 20 half + u
+  if (ok) {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      if (i >= nch) break;
+      const int k0 = half * 20 + 4 * i;
+      uint32_t ea[4], oa[4], eb[4], ob[4];
+      ADMP_TC_LD4(dre + lane_base + k0, ea);
+      ADMP_TC_LD4(dre + lane_base + 40 + k0, oa);
+      ADMP_TC_LD4(dim + lane_base + k0, eb);
+      ADMP_TC_LD4(dim + lane_base + 40 + k0, ob);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      float ur[4], ui[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = k0 + u;
+        const float Ea = __uint_as_float(ea[u]), Oa = __uint_as_float(oa[u]);
+        const float Eb = __uint_as_float(eb[u]), Ob = __uint_as_float(ob[u]);
+        const float ga = g1[4 * i + u], gb = g2[4 * i + u];
+        if (k == 0 || 2 * k == K0) {  // stands alone: S = (Ea, Eb)
+          ur[u] = ga * Ea;
+          ui[u] = ga * Eb;
+          wr[4 * i + u] = 0.f;
+          wi[4 * i + u] = 0.f;
+        } else {  // zero past K0 / 2 through g
+          const float t1r = ga * (Ea + Ob), t1i = ga * (Eb - Oa);
+          const float t2r = gb * (Ea - Ob), t2i = gb * (Eb + Oa);
+          ur[u] = t1r + t2r;
+          ui[u] = t1i + t2i;
+          wr[4 * i + u] = t1r - t2r;
+          wi[4 * i + u] = t2i - t1i;
+        }
+      }
+      tc_put4(Arh, Arl, row, k0, ur);
+      tc_put4(Aih, Ail, row, k0, ui);
+    }
+  }
+  // chunks past K0 / 2 (and every chunk after a failed wait) hold no input: zero
+  auto zero_rest = [&]() {
+    for (int it = tid; it < kTcRows * (kTcHalf / 4); it += 256) {
+      const int r = it & (kTcRows - 1), k4 = (it >> 7) * 4;
+      if (ok && k4 <= h0) continue;
+      const float z[4] = {0.f, 0.f, 0.f, 0.f};
+      tc_put4(Arh, Arl, r, k4, z);
+      tc_put4(Aih, Ail, r, k4, z);
+    }
+  };
+  zero_rest();
+  publish();
+  // stage 3, U half: out = U Phi^T (cos columns); N = x rows, 16-aligned past K0
+  const int n3 = ((K0 + 15) >> 4) << 4;
+  run_half((h0 + 1 + 7) >> 3, n3, false);
+  await_half();
+  // V half (sin columns; V_0 = 0 and V is zero past (K0 - 1) / 2)
+  if (ns >= 1) {
+    if (tid == 0 && ok) tc_load_b(Bt, tb + 6 * (size_t)kTcImgWords, &bar_b);  // stage 3, j' >= 40
     if (ok) {
-      // epilogue 3: x in [40 half, 40 half + 40), eight at a time
-      Cplx<float>* Ho = spec + cur.spec_off + c;
 #pragma unroll
       for (int i = 0; i < 5; ++i) {
-        const int x0 = half * 40 + 8 * i;
-        if (x0 >= K0) break;  // block-uniform
-        uint32_t vr[8], vi[8];
-        ADMP_TC_LD8(dre + lane_base + x0, vr);
-        ADMP_TC_LD8(dim + lane_base + x0, vi);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (live)
+        if (i >= nch) break;
+        const int k0 = half * 20 + 4 * i;
+        float a[4], bq[4];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const int x = x0 + u;
-            if (x < K0) {
-              Cplx<float> o;
-              o.x = __uint_as_float(vr[u]);
-              o.y = __uint_as_float(vi[u]);
-              Ho[(size_t)x * xs] = o;
-            }
-          }
+        for (int u = 0; u < 4; ++u) {
+          a[u] = wi[4 * i + u];
+          bq[u] = wr[4 * i + u];
+        }
+        tc_put4(Arh, Arl, row, k0, a);   // re row: -V_im
+        tc_put4(Aih, Ail, row, k0, bq);  // im row:  V_re
       }
-    } else if (tid == 0 && b.done) {
-      atomicExch(const_cast<int*>(b.done) + (size_t)cur.box_idx * b.done_stride + b.status_off, ADMP_ERR_CUDA);
     }
+    zero_rest();
+    publish();
+    run_half((ns + 1 + 7) >> 3, n3, true);
+    await_half();
+  }
+  if (ok) {
+    // epilogue: x in [40 half, 40 half + 40), eight at a time
+    Cplx<float>* Ho = spec + cur.spec_off + c;
+    const int nx = K0 > half * 40 ? min(5, (K0 - half * 40 + 7) / 8) : 0;  // block-uniform
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      if (i >= nx) break;
+      const int x0 = half * 40 + 8 * i;
+      uint32_t vr[8], vi[8];
+      ADMP_TC_LD8(dre + lane_base + x0, vr);
+      ADMP_TC_LD8(dim + lane_base + x0, vi);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (live)
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int x = x0 + u;
+          if (x < K0) {
+            Cplx<float> o;
+            o.x = __uint_as_float(vr[u]);
+            o.y = __uint_as_float(vi[u]);
+            Ho[(size_t)x * xs] = o;
+          }
+        }
+    }
+  } else if (tid == 0 && b.done) {
+    atomicExch(const_cast<int*>(b.done) + (size_t)cur.box_idx * b.done_stride + b.status_off, ADMP_ERR_CUDA);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

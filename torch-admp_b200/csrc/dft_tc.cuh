@@ -428,4 +428,394 @@ static __global__ void __launch_bounds__(256, 2)
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tm));
 }
 
+// y pass (forward, or inverse through conjugation: IDFT(h) = conj(DFT(conj(h)))) of the FP32 CG
+// matvec on the tensor cores, in place on the half spectrum H[x][y][kz]: a tile is 128 lines
+// r = (x, kz) of one system, line r holding H[x][.][kz] (stride K2h); stage 1 of the x pass without
+// the Green's function and stage 3.  Two CTAs per SM.
+template <bool INV>
+static __global__ void __launch_bounds__(256, 2)
+    tc_y_kernel(Batch b, Cplx<float>* __restrict__ spec, const uint32_t* __restrict__ tab) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  __shared__ __align__(8) uint64_t bar_b, bar_m;
+  __shared__ uint32_t tslot;
+  unsigned char* Arh = tsm;
+  unsigned char* Arl = Arh + kTcATile;
+  unsigned char* Aih = Arl + kTcATile;
+  unsigned char* Ail = Aih + kTcATile;
+  unsigned char* Bt = Ail + kTcATile;  // head, tail
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int s = find_sys<F_YT>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K1 = d.K1, K2h = d.K2h, h1 = K1 / 2;
+  const int r0 = (blockIdx.x - d.blk_yt) * kTcRows, nz = min(kTcRows, d.K0 * K2h - r0);
+  const size_t ys = (size_t)K2h, plane = (size_t)K1 * K2h;
+  Cplx<float>* H = spec + d.spec_off;
+  const FastDiv fk = fast_div(K2h);
+  const uint32_t* tb = tab + (size_t)K1 * 8 * kTcImgWords;  // [part][head, tail]
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar_b)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar_m)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tc_load_b(Bt, tb, &bar_b);  // y < 40
+  }
+  __syncwarp();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(tc_smem(&tslot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // the tile's lines as rows, y as columns (every load of a thread in flight before the first use)
+  Cplx<float> v[10][4];
+  {
+    const int ca = tid & (kTcRows - 1), ya = (tid >> 7) * 4;
+    const bool la = ca < nz;
+    const int r = r0 + (la ? ca : 0), x = fdiv(r, fk);
+    const Cplx<float>* L = H + (size_t)x * plane + (r - x * K2h);
+#pragma unroll
+    for (int m = 0; m < 10; ++m)
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int y = ya + 8 * m + t;
+        v[m][t].x = 0.f;
+        v[m][t].y = 0.f;
+        if (la && y < K1) v[m][t] = L[(size_t)y * ys];
+        if (INV) v[m][t].y = -v[m][t].y;
+      }
+  }
+  tc_stage_a<0>(Arh, Arl, Aih, Ail, tid, v);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tm = tslot;
+  const uint32_t dre = tm, dim = tm + 128;
+  const int q = warp & 3, half = warp >> 2, row = q * 32 + lane;
+  const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+  uint32_t pb = 0, pm = 0;
+  bool ok = true;
+  auto run_half = [&](int ks, bool acc) {
+    if (tid == 0 && ok) {
+      ok = tc_wait(&bar_b, pb & 1);
+      if (ok) {
+        tc_products(dre, dim, Arh, Arl, Aih, Ail, Bt, ks, kTcN, acc);
+        tc_commit(&bar_m);
+      }
+    }
+    ++pb;
+  };
+  auto await_half = [&]() {
+    ok = __syncthreads_and(ok) != 0;
+    ok = __syncthreads_and(ok && tc_wait(&bar_m, pm & 1)) != 0;
+    ++pm;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  };
+  run_half(min(5, (K1 + 7) >> 3), false);
+  await_half();
+  if (K1 > kTcHalf) {
+    if (tid == 0 && ok) tc_load_b(Bt, tb + 2 * (size_t)kTcImgWords, &bar_b);  // y >= 40
+    tc_stage_a<5>(Arh, Arl, Aih, Ail, tid, v);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    run_half((K1 - kTcHalf + 7) >> 3, true);
+    await_half();
+  }
+  if (ok) {
+    // S_k = Ea + Ob + i (Eb - Oa) for k <= K1 / 2, S_{K1-k} = Ea - Ob + i (Eb + Oa) for 1 <= k < K1 / 2
+    // (the sine columns of k = 0 and of the Nyquist index are zero)
+    const bool live = row < nz;
+    const int r = r0 + (live ? row : 0), x = fdiv(r, fk);
+    Cplx<float>* L = H + (size_t)x * plane + (r - x * K2h);
+    const int nch = h1 >= half * 20 ? min(5, (h1 - half * 20) / 4 + 1) : 0;  // block-uniform
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      if (i >= nch) break;
+      const int k0 = half * 20 + 4 * i;
+      uint32_t ea[4], oa[4], eb[4], ob[4];
+      ADMP_TC_LD4(dre + lane_base + k0, ea);
+      ADMP_TC_LD4(dre + lane_base + 40 + k0, oa);
+      ADMP_TC_LD4(dim + lane_base + k0, eb);
+      ADMP_TC_LD4(dim + lane_base + 40 + k0, ob);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (live)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = k0 + u;
+          if (k > h1) break;
+          const float Ea = __uint_as_float(ea[u]), Oa = __uint_as_float(oa[u]);
+          const float Eb = __uint_as_float(eb[u]), Ob = __uint_as_float(ob[u]);
+          Cplx<float> o;
+          o.x = Ea + Ob;
+          o.y = INV ? Oa - Eb : Eb - Oa;
+          L[(size_t)k * ys] = o;
+          if (k >= 1 && 2 * k != K1) {
+            o.x = Ea - Ob;
+            o.y = INV ? -(Eb + Oa) : Eb + Oa;
+            L[(size_t)(K1 - k) * ys] = o;
+          }
+        }
+    }
+  } else if (tid == 0 && b.done) {
+    atomicExch(const_cast<int*>(b.done) + (size_t)d.box_idx * b.done_stride + b.status_off, ADMP_ERR_CUDA);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tm));
+}
+
+// Products of a real operand: D += A B over ks K-steps, head*head + head*tail + tail*head.
+__device__ __forceinline__ void tc_products_real(uint32_t dt, const unsigned char* Ah, const unsigned char* Al,
+                                                 const unsigned char* Bt, int ks, int n, bool acc) {
+  const uint32_t id = tc_idesc(n);
+  const uint64_t ah = tc_desc(tc_smem(Ah)), al = tc_desc(tc_smem(Al)), bh = tc_desc(tc_smem(Bt)),
+                 bl = tc_desc(tc_smem(Bt + kTcBTile));
+  for (int k = 0; k < ks; ++k) {
+    const uint64_t o = (uint64_t)k * 16;
+    tc_mma(dt, ah + o, bh + o, id, (acc || k > 0) ? 1u : 0u);
+    tc_mma(dt, ah + o, bl + o, id, 1u);
+    tc_mma(dt, al + o, bh + o, id, 1u);
+  }
+}
+
+// Shared state of the z passes: a tile is 128 lines r = (x, y) of one system (contiguous in both
+// the mesh, K2 reals a line, and the half spectrum, K2h complex a line), staged through shared
+// memory so that global loads and stores are coalesced.  Layout: A head / tail (one 40-column half),
+// the staging area (40 KB), B head / tail.  TMEM: one accumulator of 128 columns.
+struct TcZ {
+  unsigned char *Ah, *Al, *Bt;
+  float* S;
+  uint64_t *bar_b, *bar_m;
+  uint32_t tm;
+  uint32_t pb, pm;
+  bool ok;
+};
+
+__device__ __forceinline__ void tc_z_half(TcZ& z, int tid, int ks, int n, bool acc) {
+  if (tid == 0 && z.ok) {
+    z.ok = tc_wait(z.bar_b, z.pb & 1);
+    if (z.ok) {
+      tc_products_real(z.tm, z.Ah, z.Al, z.Bt, ks, n, acc);
+      tc_commit(z.bar_m);
+    }
+  }
+  ++z.pb;
+  z.ok = __syncthreads_and(z.ok) != 0;
+  z.ok = __syncthreads_and(z.ok && tc_wait(z.bar_m, z.pm & 1)) != 0;
+  ++z.pm;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_publish() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// z pass forward (real to half spectrum): H[r][kz] = sum_z q[r][z] (cos - i sin)(2 pi z kz / K2),
+// i.e. D = A Phi with the cosine columns kz and the sine columns 40 + kz.  Two CTAs per SM.
+static __global__ void __launch_bounds__(256, 2)
+    tc_zf_kernel(Batch b, const float* __restrict__ mesh, Cplx<float>* __restrict__ spec,
+                 const uint32_t* __restrict__ tab) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  __shared__ __align__(8) uint64_t bar_b, bar_m;
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int s = find_sys<F_ZT>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K2 = d.K2, K2h = d.K2h;
+  const int r0 = (blockIdx.x - d.blk_zt) * kTcRows, nz = min(kTcRows, d.K0 * d.K1 - r0);
+  TcZ z;
+  z.Ah = tsm;
+  z.Al = z.Ah + kTcATile;
+  z.S = reinterpret_cast<float*>(z.Al + kTcATile);
+  z.Bt = z.Al + 3 * kTcATile;
+  z.bar_b = &bar_b;
+  z.bar_m = &bar_m;
+  z.pb = z.pm = 0;
+  z.ok = true;
+  const uint32_t* tb = tab + (size_t)K2 * 8 * kTcImgWords;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar_b)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar_m)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tc_load_b(z.Bt, tb, &bar_b);  // z < 40
+  }
+  __syncwarp();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(tc_smem(&tslot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  {
+    const float* Q = mesh + d.mesh_off + (size_t)r0 * K2;
+    const int n = nz * K2;
+    for (int i = tid; i < n; i += 256) z.S[i] = Q[i];
+  }
+  __syncthreads();
+  z.tm = tslot;
+  const int ca = tid & (kTcRows - 1), za = (tid >> 7) * 4;
+  auto fill = [&](int hh) {
+#pragma unroll
+    for (int mm = 0; mm < 5; ++mm) {
+      float v[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int zz = kTcHalf * hh + za + 8 * mm + t;
+        v[t] = (ca < nz && zz < K2) ? z.S[ca * K2 + zz] : 0.f;
+      }
+      tc_put4(z.Ah, z.Al, ca, za + 8 * mm, v);
+    }
+  };
+  fill(0);
+  tc_publish();
+  tc_z_half(z, tid, min(5, (K2 + 7) >> 3), kTcN, false);
+  if (K2 > kTcHalf) {
+    if (tid == 0 && z.ok) tc_load_b(z.Bt, tb + 2 * (size_t)kTcImgWords, &bar_b);  // z >= 40
+    fill(1);
+    tc_publish();
+    tc_z_half(z, tid, (K2 - kTcHalf + 7) >> 3, kTcN, true);
+  }
+  // D -> H (cos, -sin) into the staging area as [row][kz], then coalesced stores
+  const int q = warp & 3, half = warp >> 2, row = q * 32 + lane;
+  const uint32_t lb = z.tm + ((uint32_t)(q * 32) << 16);
+  Cplx<float>* Sc = reinterpret_cast<Cplx<float>*>(z.S);
+  if (z.ok) {
+    const int nch = K2h - 1 >= half * 20 ? min(5, (K2h - 1 - half * 20) / 4 + 1) : 0;  // block-uniform
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      if (i >= nch) break;
+      const int k0 = half * 20 + 4 * i;
+      uint32_t c4[4], s4[4];
+      ADMP_TC_LD4(lb + k0, c4);
+      ADMP_TC_LD4(lb + 40 + k0, s4);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = k0 + u;
+        if (k < K2h) {
+          Cplx<float> o;
+          o.x = __uint_as_float(c4[u]);
+          o.y = -__uint_as_float(s4[u]);
+          Sc[row * K2h + k] = o;
+        }
+      }
+    }
+  } else if (tid == 0 && b.done) {
+    atomicExch(const_cast<int*>(b.done) + (size_t)d.box_idx * b.done_stride + b.status_off, ADMP_ERR_CUDA);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (z.ok) {
+    Cplx<float>* H = spec + d.spec_off + (size_t)r0 * K2h;
+    const int n = nz * K2h;
+    for (int i = tid; i < n; i += 256) H[i] = Sc[i];
+  }
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(z.tm));
+}
+
+// z pass inverse (half spectrum to real, unnormalised): q[r][z] = sum_k w_k (Re S_k cos - Im S_k sin)
+// with w = 1 at k = 0 and at the Nyquist index, 2 elsewhere, i.e. A = [w Re S | -w Im S] and
+// q = A Phi^T (the cosine half, then the sine half).  Two CTAs per SM.
+static __global__ void __launch_bounds__(256, 2)
+    tc_zi_kernel(Batch b, const Cplx<float>* __restrict__ spec, float* __restrict__ mesh,
+                 const uint32_t* __restrict__ tab) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  __shared__ __align__(8) uint64_t bar_b, bar_m;
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int s = find_sys<F_ZT>(b, blockIdx.x);
+  if (skip_sys(b, s)) return;
+  const SysDesc& d = b.s[s];
+  const int K2 = d.K2, K2h = d.K2h, ns = (K2 - 1) / 2;
+  const int r0 = (blockIdx.x - d.blk_zt) * kTcRows, nz = min(kTcRows, d.K0 * d.K1 - r0);
+  TcZ z;
+  z.Ah = tsm;
+  z.Al = z.Ah + kTcATile;
+  z.S = reinterpret_cast<float*>(z.Al + kTcATile);
+  z.Bt = z.Al + 3 * kTcATile;
+  z.bar_b = &bar_b;
+  z.bar_m = &bar_m;
+  z.pb = z.pm = 0;
+  z.ok = true;
+  const uint32_t* tb = tab + (size_t)K2 * 8 * kTcImgWords;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar_b)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar_m)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tc_load_b(z.Bt, tb + 4 * (size_t)kTcImgWords, &bar_b);  // cosine columns
+  }
+  __syncwarp();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(tc_smem(&tslot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  Cplx<float>* Sc = reinterpret_cast<Cplx<float>*>(z.S);
+  {
+    const Cplx<float>* H = spec + d.spec_off + (size_t)r0 * K2h;
+    const int n = nz * K2h;
+    for (int i = tid; i < n; i += 256) Sc[i] = H[i];
+  }
+  __syncthreads();
+  z.tm = tslot;
+  const int ca = tid & (kTcRows - 1), ka = (tid >> 7) * 4;
+  // hh = 0: w Re S_k at column k (k <= K2 / 2); hh = 1: -w Im S_k at column k (1 <= k <= ns)
+  auto fill = [&](int hh) {
+#pragma unroll
+    for (int mm = 0; mm < 5; ++mm) {
+      float v[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int k = ka + 8 * mm + t;
+        const bool in = ca < nz && (hh == 0 ? k < K2h : (k >= 1 && k <= ns));
+        const float w = (k == 0 || 2 * k == K2) ? 1.f : 2.f;
+        v[t] = 0.f;
+        if (in) {
+          const Cplx<float> e = Sc[ca * K2h + k];
+          v[t] = hh == 0 ? w * e.x : -w * e.y;
+        }
+      }
+      tc_put4(z.Ah, z.Al, ca, ka + 8 * mm, v);
+    }
+  };
+  const int n3 = ((K2 + 15) >> 4) << 4;
+  fill(0);
+  tc_publish();
+  tc_z_half(z, tid, (K2h + 7) >> 3, n3, false);
+  if (ns >= 1) {
+    if (tid == 0 && z.ok) tc_load_b(z.Bt, tb + 6 * (size_t)kTcImgWords, &bar_b);  // sine columns
+    fill(1);
+    tc_publish();
+    tc_z_half(z, tid, (ns + 1 + 7) >> 3, n3, true);
+  }
+  // D -> q[row][z] into the staging area, then coalesced stores
+  const int q = warp & 3, half = warp >> 2, row = q * 32 + lane;
+  const uint32_t lb = z.tm + ((uint32_t)(q * 32) << 16);
+  if (z.ok) {
+    const int nx = K2 > half * 40 ? min(5, (K2 - half * 40 + 7) / 8) : 0;  // block-uniform
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      if (i >= nx) break;
+      const int z0 = half * 40 + 8 * i;
+      uint32_t v8[8];
+      ADMP_TC_LD8(lb + z0, v8);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (z0 + u < K2) z.S[row * K2 + z0 + u] = __uint_as_float(v8[u]);
+    }
+  } else if (tid == 0 && b.done) {
+    atomicExch(const_cast<int*>(b.done) + (size_t)d.box_idx * b.done_stride + b.status_off, ADMP_ERR_CUDA);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (z.ok) {
+    float* Q = mesh + d.mesh_off + (size_t)r0 * K2;
+    const int n = nz * K2;
+    for (int i = tid; i < n; i += 256) Q[i] = z.S[i];
+  }
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(z.tm));
+}
+
 }  // namespace admp

@@ -31,8 +31,10 @@ struct RecipPlan {
   bool slab = false;
   int buf_elems = 0;
   size_t smem_slab = 0;
-  // FP32 CG matvecs: x pass on the tensor cores (every K0 <= kTcMaxK)
+  // FP32 CG matvecs: x pass on the tensor cores (every K0 <= kTcMaxK), and the y and z passes too
+  // (every K1, K2 <= kTcMaxK)
   bool tc_x = false;
+  bool tc_y = false;
 };
 
 // The per-system table as one by-value parameter: the only launch of a call
@@ -73,6 +75,8 @@ inline Batch family_batch(const RecipPlan<T>& p, int F) {
                : F == F_Y  ? d.blk_y
                : F == F_X  ? d.blk_x
                : F == F_XT ? d.blk_xt
+               : F == F_YT ? d.blk_yt
+               : F == F_ZT ? d.blk_zt
                            : d.blk_slab;
   }
   return b;
@@ -117,7 +121,7 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
   p.smem_x = (2 * (size_t)zb + 1) * maxK[0] * cs + ((size_t)maxK[0] + 2 * zb) * 8 + (size_t)zb * 16;
   if (p.smem_z > 227 * 1024 || p.smem_y > 227 * 1024 || p.smem_x > 227 * 1024)
     return fail(ADMP_ERR_MESH, "mesh %dx%dx%d too large for the shared-memory FFT", maxK[0], maxK[1], maxK[2]);
-  int ba = 0, bz = 0, by = 0, bx = 0, bxt = 0;
+  int ba = 0, bz = 0, by = 0, bx = 0, bxt = 0, byt = 0, bzt = 0;
   size_t mo = 0, so = 0;
   for (int s = 0; s < nsys; ++s) {
     SysDesc& d = p.hs[s];
@@ -135,6 +139,8 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
     d.blk_y = by;
     d.blk_x = bx;
     d.blk_xt = bxt;
+    d.blk_yt = byt;
+    d.blk_zt = bzt;
     d.mesh_off = (int64_t)mo;
     d.spec_off = (int64_t)so;
     d.green_off = sys[s].green_off >= 0 ? (int64_t)sys[s].green_off : (int64_t)so;
@@ -144,12 +150,17 @@ inline int build_recip_plan(const SysSpec* sys, int nsys, RecipPlan<T>& p) {
     by += d.K0 * ncb;
     bx += (d.K1 * d.K2h + zb - 1) / zb;  // x passes: runs of zb flattened (y, kz) columns
     bxt += (d.K1 * d.K2h + kTcRows - 1) / kTcRows;
+    byt += (d.K0 * d.K2h + kTcRows - 1) / kTcRows;
+    bzt += (d.K0 * d.K1 + kTcRows - 1) / kTcRows;
     mo += align_up((size_t)d.K0 * d.K1 * d.K2, 64);
     so += align_up((size_t)d.K0 * d.K1 * d.K2h, 32);
   }
   b.nblk_atom = ba;
   b.nblk_xt = bxt;
+  b.nblk_yt = byt;
+  b.nblk_zt = bzt;
   p.tc_x = sizeof(T) == 4 && maxK[0] <= kTcMaxK;
+  p.tc_y = p.tc_x && maxK[1] <= kTcMaxK && maxK[2] <= kTcMaxK;
   b.nblk_z = bz;
   b.nblk_y = by;
   b.nblk_x = bx;
@@ -202,6 +213,37 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
   // algorithmic bytes: z passes read/write M reals + Mh complex, y/x passes Mh complex in and out
   const double rb = (double)p.mesh_elems * sizeof(T), cb = (double)p.spec_elems * sizeof(Cplx<T>);
   int h;
+  // FP32 CG matvecs on the tensor cores: every pass a matrix product
+  const uint32_t* tct = (green && p.tc_x) ? tc_tables(st) : nullptr;
+  if (tct) ADMP_CUDA_TRY(ensure_smem(tc_x_apply_kernel, (size_t)kTcSmem));
+  if (tct && p.tc_y) {
+    ADMP_CUDA_TRY(ensure_smem(tc_y_kernel<false>, (size_t)kTcSmem));
+    ADMP_CUDA_TRY(ensure_smem(tc_y_kernel<true>, (size_t)kTcSmem));
+    ADMP_CUDA_TRY(ensure_smem(tc_zf_kernel, (size_t)kTcSmem));
+    ADMP_CUDA_TRY(ensure_smem(tc_zi_kernel, (size_t)kTcSmem));
+    const Batch bzt = family_batch(p, F_ZT);
+    Cplx<float>* sp = (Cplx<float>*)spec;
+    const Batch byt = family_batch(p, F_YT);
+    h = prof_begin(st);
+    if (b.nblk_zt) tc_zf_kernel<<<b.nblk_zt, 256, kTcSmem, st>>>(bzt, (const float*)mesh, sp, tct);
+    prof_end(h, PK_FFT_Z_FWD, rb + cb, st);
+    h = prof_begin(st);
+    if (b.nblk_yt) tc_y_kernel<false><<<b.nblk_yt, 256, kTcSmem, st>>>(byt, sp, tct);
+    prof_end(h, PK_FFT_Y_FWD, 2 * cb, st);
+    h = prof_begin(st);
+    if (b.nblk_xt)
+      tc_x_apply_kernel<<<b.nblk_xt, 256, kTcSmem, st>>>(family_batch(p, F_XT), sp, (const float*)green, tct);
+    prof_end(h, PK_FFT_X_GREEN, 2 * cb + (double)p.spec_elems * sizeof(T), st);
+    h = prof_begin(st);
+    if (b.nblk_yt) tc_y_kernel<true><<<b.nblk_yt, 256, kTcSmem, st>>>(byt, sp, tct);
+    prof_end(h, PK_FFT_Y_INV, 2 * cb, st);
+    h = prof_begin(st);
+    if (b.nblk_zt) tc_zi_kernel<<<b.nblk_zt, 256, kTcSmem, st>>>(bzt, sp, (float*)mesh, tct);
+    prof_end(h, PK_FFT_Z_INV, rb + cb, st);
+    count_launches(5);
+    ADMP_CUDA_TRY(cudaGetLastError());
+    return ADMP_OK;
+  }
   if (p.slab) {
     ADMP_CUDA_TRY(ensure_smem(fft_slab_fwd_kernel<T>, p.smem_slab));
     ADMP_CUDA_TRY(ensure_smem(fft_slab_inv_kernel<T>, p.smem_slab));
@@ -216,8 +258,6 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
     if (b.nblk_y) fft_y_kernel<T, false><<<b.nblk_y, 256, p.smem_y, st>>>(by, spec);
     prof_end(h, PK_FFT_Y_FWD, 2 * cb, st);
   }
-  const uint32_t* tct = (green && p.tc_x) ? tc_tables(st) : nullptr;
-  if (tct) ADMP_CUDA_TRY(ensure_smem(tc_x_apply_kernel, (size_t)kTcSmem));
   h = prof_begin(st);
   if (b.nblk_x) {
     if (tct)

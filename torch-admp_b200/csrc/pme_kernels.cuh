@@ -23,6 +23,8 @@ struct SysDesc {
   int32_t K0, K1, K2, K2h;
   int32_t blk_atom, blk_z, blk_y, blk_x, blk_slab;
   int32_t blk_xt;  // first block of the tensor-core x pass (128 columns per block)
+  int32_t blk_yt;  // first block of the tensor-core y passes (128 (x, kz) lines per block)
+  int32_t blk_zt;  // first block of the tensor-core z passes (128 (x, y) lines per block)
   int64_t mesh_off, spec_off;
   int64_t green_off;  // cached 2 G_s (half-spectrum layout) for CG matvecs
   double kappa;
@@ -36,7 +38,7 @@ struct SysDesc {
 // of a call do not each carry the whole table as a kernel parameter).
 struct Batch {
   int nsys;
-  int nblk_atom, nblk_z, nblk_y, nblk_x, nblk_slab, nblk_xt;
+  int nblk_atom, nblk_z, nblk_y, nblk_x, nblk_slab, nblk_xt, nblk_yt, nblk_zt;
   int apb;  // atoms per block (atom kernels)
   int lp;   // line pairs per block (z passes)
   int zb;   // columns per block (y / x passes)
@@ -64,7 +66,7 @@ constexpr int kAccVk = 1;       // 9: dE/dB (B = box^-1) through k vectors
 constexpr int kAccWf = 10;      // 9: dE/dB through fractional coordinates
 constexpr int kAccSlots = 19;
 
-enum SysField { F_ATOM = 0, F_Z = 1, F_Y = 2, F_X = 3, F_SLAB = 4, F_XT = 5 };
+enum SysField { F_ATOM = 0, F_Z = 1, F_Y = 2, F_X = 3, F_SLAB = 4, F_XT = 5, F_YT = 6, F_ZT = 7 };
 
 template <int F>
 __device__ __forceinline__ int blk_of(const SysDesc& d) {
@@ -73,6 +75,8 @@ __device__ __forceinline__ int blk_of(const SysDesc& d) {
          : F == F_Y  ? d.blk_y
          : F == F_X  ? d.blk_x
          : F == F_XT ? d.blk_xt
+         : F == F_YT ? d.blk_yt
+         : F == F_ZT ? d.blk_zt
                      : d.blk_slab;
 }
 

@@ -578,6 +578,16 @@ __device__ __forceinline__ void tc_products_real(uint32_t dt, const unsigned cha
   }
 }
 
+// Asynchronous global -> shared copies of 4 or 8 bytes (cp.async, no register round trip): a thread
+// issues all of its copies before waiting, so the staging of a tile is one memory latency.
+template <int BYTES>
+__device__ __forceinline__ void tc_cp_async(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(tc_smem(smem)), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void tc_cp_async_wait() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Shared state of the z passes: a tile is 128 lines r = (x, y) of one system (contiguous in both
 // the mesh, K2 reals a line, and the half spectrum, K2h complex a line), staged through shared
 // memory so that global loads and stores are coalesced.  Layout: A head / tail (one 40-column half),
@@ -651,7 +661,8 @@ static __global__ void __launch_bounds__(256, 2)
   {
     const float* Q = mesh + d.mesh_off + (size_t)r0 * K2;
     const int n = nz * K2;
-    for (int i = tid; i < n; i += 256) z.S[i] = Q[i];
+    for (int i = tid; i < n; i += 256) tc_cp_async<4>(z.S + i, Q + i);
+    tc_cp_async_wait();
   }
   __syncthreads();
   z.tm = tslot;
@@ -755,7 +766,8 @@ static __global__ void __launch_bounds__(256, 2)
   {
     const Cplx<float>* H = spec + d.spec_off + (size_t)r0 * K2h;
     const int n = nz * K2h;
-    for (int i = tid; i < n; i += 256) Sc[i] = H[i];
+    for (int i = tid; i < n; i += 256) tc_cp_async<8>(Sc + i, H + i);
+    tc_cp_async_wait();
   }
   __syncthreads();
   z.tm = tslot;

@@ -165,7 +165,9 @@ __device__ __forceinline__ void tc_put4(unsigned char* hi, unsigned char* lo, in
 // The B images of every mesh length 1..kTcMaxK, [K0][part][head, tail][kTcImgWords] with parts
 // 0, 1 = stage 1 (Phi^T restricted to x < 40, x >= 40) and 2, 3 = stage 3 (Phi restricted to
 // j' < 40, j' >= 40) (dft_tc.cu): built on the current device at the first call (ordered on `st`
-// and waited for, so any stream may read them afterwards).  nullptr if they cannot be built.
+// and waited for, so any stream may read them afterwards).  nullptr if they cannot be built.  The first
+// call on a device synchronises `st` (not allowed while `st` is being captured into a CUDA graph: make
+// one uncaptured call first); the cached address is not valid across cudaDeviceReset.
 const uint32_t* tc_tables(cudaStream_t st);
 
 // One tile: 128 flattened columns of one system (block family F_XT).

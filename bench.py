@@ -339,6 +339,57 @@ def accuracy_vs(results, ref):
             "requests": len(ref)}
 
 
+def tc_matvec_flops(km) -> float:
+    """Tensor-core FLOPs of one FP32 CG matvec's mesh passes on a K0 x K1 x K2 mesh, as the kernels
+    issue them: 128-line tiles, 8-column K-steps, three TF32 products per step (head / tail split),
+    padding included (csrc/dft_tc.cuh)."""
+    K0, K1, K2 = (int(k) for k in km)
+    K2h = K2 // 2 + 1
+
+    def cd(a, b):
+        return -(-a // b)
+
+    def ks(K):  # K-steps of a contraction over K in two 40-column halves
+        return min(5, cd(K, 8)) + (cd(K - 40, 8) if K > 40 else 0)
+
+    def step(n):  # one 3-term K-step: 128 x n x 8 products
+        return 3 * 2 * 128 * n * 8
+
+    tz, ty, tx = cd(K0 * K1, 128), cd(K0 * K2h, 128), cd(K1 * K2h, 128)
+    n0, n2 = cd(K0, 16) * 16, cd(K2, 16) * 16
+    ns0, ns2 = (K0 - 1) // 2, (K2 - 1) // 2
+    zf = tz * ks(K2) * step(80)
+    y = ty * 2 * ks(K1) * step(80)
+    x = tx * 2 * (ks(K0) * step(80) + (cd(K0 // 2 + 1, 8) + (cd(ns0 + 1, 8) if ns0 >= 1 else 0)) * step(n0))
+    zi = tz * (cd(K2h, 8) + (cd(ns2 + 1, 8) if ns2 >= 1 else 0)) * step(n2)
+    return float(zf + 2 * y + x + zi)
+
+
+def tensor_roofline(stream, results, prof, peaks, kap):
+    """Achieved tensor throughput of the CG matvec's mesh passes in the profiled pass: the FLOPs the
+    tensor-core kernels issue ((iterations + 1) matvecs per QEq request) over their CUDA-event time,
+    against dense TF32 = half the measured BF16 rate (the tensor cores run TF32 at half the BF16 rate)."""
+    from admp_b200.serving import auto_kmesh
+    names = ("tc_z_fwd", "tc_y_fwd", "tc_x", "tc_y_inv", "tc_z_inv")
+    ms = sum(prof[k]["ms"] for k in names if k in prof)
+    if ms <= 0:
+        return None
+    byrid = {r.rid: r for r in stream}
+    flops = 0.0
+    for res in results:
+        if res.kind != "qeq":
+            continue
+        km = auto_kmesh(np.diagonal(byrid[res.rid].box), kap, ETHRESH)
+        flops += (res.iterations + 1) * tc_matvec_flops(km)
+    achieved = flops / (ms / 1e3) / 1e12
+    bf16 = float(peaks.get("bf16_tflops", 0.0)) if peaks else 0.0
+    peak = bf16 / 2 if bf16 > 0 else 1590.0 / 2
+    return {"kernels": list(names), "ms": ms, "tflops": achieved, "peak_tflops": peak,
+            "peak_source": "half the measured bf16 burst" if bf16 > 0 else "half the fallback bf16",
+            "frac": achieved / peak,
+            "flops_note": "TF32 products as issued: three per term (head / tail split), padding included"}
+
+
 def same_sample_gpu(eng, reqs, passes: int = 3):
     """The FP32 serving engine on the CPU baseline's sample (host numpy in and
     out, as e2e): systems/s over `passes` passes after one untimed pass, and
@@ -600,7 +651,7 @@ def main():
 
     # profile pass: per-kernel device time from CUDA events on the launch stream
     L.profile_enable(200000)
-    one_pass(dstream, to_host=False)
+    pres = one_pass(dstream, to_host=False)
     torch.cuda.synchronize()
     prof = L.profile_read()
     L.profile_enable(0)
@@ -682,6 +733,7 @@ def main():
     achieved = rf[dom]["gbs"]
     alg_per_launch = achieved * 1e9 * rf[dom]["ms_per_launch"] / 1e3
     traffic = TRAFFIC_PER_ALG_BYTE[dom] * alg_per_launch if dom in TRAFFIC_PER_ALG_BYTE else None
+    tensor = tensor_roofline(stream, pres, prof, peaks, kap)
     extra = {}
     if not args.no_extra:
         extra["fp64"] = fp64_serving(stream, dev, args, world)
@@ -717,6 +769,7 @@ def main():
                          "max_rel_force_err_pme": ferr_pme, "max_rel_force_err_qeq": ferr_qeq,
                          "sample": f"first {args.plain_sample} requests vs the FP64 drop-in path "
                                    "(QEq solved to ||P grad||/N < 1e-10)"},
+            "tensor_passes": tensor,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "traffic_source": ("ncu DRAM bytes per algorithmic byte of the 400-request stream "

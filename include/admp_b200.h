@@ -78,8 +78,11 @@ long long admp_launch_count(void);
  * hot kernels are bracketed by CUDA events on their launch stream and tagged
  * with their algorithmic bytes.  admp_profile_read fills per-kernel totals
  * (index order: spread, fft_z_fwd, fft_y_fwd, fft_x_green, fft_y_inv,
- * fft_z_inv, gather, pair_ef, csr_spmv, neighbors, cg_vector). */
-#define ADMP_PROFILE_KERNELS 12
+ * fft_z_inv, gather, pair_ef, csr_spmv, neighbors, cg_vector, tc_z_fwd,
+ * tc_y_fwd, tc_x, tc_y_inv, tc_z_inv; the tc_* entries are the FP32 CG
+ * matvec's mesh passes on the tensor cores, the fft_* ones the shared-memory
+ * FFT passes). */
+#define ADMP_PROFILE_KERNELS 16
 int admp_profile_enable(int capacity);
 int admp_profile_read(double* ms, long long* launches, double* bytes, int n);
 

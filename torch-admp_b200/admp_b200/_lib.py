@@ -50,7 +50,7 @@ EXPORTS = [
     "admp_image_nblist_fill", "admp_image_pair_distances", "admp_image_pair_distances_backward",
 ]
 PROFILE_KERNELS = ["spread", "fft_z_fwd", "fft_y_fwd", "fft_x_green", "fft_y_inv", "fft_z_inv", "gather", "pair_ef",
-                   "csr_spmv", "neighbors", "cg_vector"]
+                   "csr_spmv", "neighbors", "cg_vector", "tc_z_fwd", "tc_y_fwd", "tc_x", "tc_y_inv", "tc_z_inv"]
 
 _vp, _i, _ll, _d, _sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double, ctypes.c_size_t
 _ip = ctypes.POINTER(ctypes.c_int)

@@ -226,20 +226,20 @@ inline int launch_fft_green(const RecipPlan<T>& p, T* mesh, Cplx<T>* spec, const
     const Batch byt = family_batch(p, F_YT);
     h = prof_begin(st);
     if (b.nblk_zt) tc_zf_kernel<<<b.nblk_zt, 256, kTcSmem, st>>>(bzt, (const float*)mesh, sp, tct);
-    prof_end(h, PK_FFT_Z_FWD, rb + cb, st);
+    prof_end(h, PK_TC_Z_FWD, rb + cb, st);
     h = prof_begin(st);
     if (b.nblk_yt) tc_y_kernel<false><<<b.nblk_yt, 256, kTcSmem, st>>>(byt, sp, tct);
-    prof_end(h, PK_FFT_Y_FWD, 2 * cb, st);
+    prof_end(h, PK_TC_Y_FWD, 2 * cb, st);
     h = prof_begin(st);
     if (b.nblk_xt)
       tc_x_apply_kernel<<<b.nblk_xt, 256, kTcSmem, st>>>(family_batch(p, F_XT), sp, (const float*)green, tct);
-    prof_end(h, PK_FFT_X_GREEN, 2 * cb + (double)p.spec_elems * sizeof(T), st);
+    prof_end(h, PK_TC_X, 2 * cb + (double)p.spec_elems * sizeof(T), st);
     h = prof_begin(st);
     if (b.nblk_yt) tc_y_kernel<true><<<b.nblk_yt, 256, kTcSmem, st>>>(byt, sp, tct);
-    prof_end(h, PK_FFT_Y_INV, 2 * cb, st);
+    prof_end(h, PK_TC_Y_INV, 2 * cb, st);
     h = prof_begin(st);
     if (b.nblk_zt) tc_zi_kernel<<<b.nblk_zt, 256, kTcSmem, st>>>(bzt, sp, (float*)mesh, tct);
-    prof_end(h, PK_FFT_Z_INV, rb + cb, st);
+    prof_end(h, PK_TC_Z_INV, rb + cb, st);
     count_launches(5);
     ADMP_CUDA_TRY(cudaGetLastError());
     return ADMP_OK;

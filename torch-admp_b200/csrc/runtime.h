@@ -27,7 +27,9 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // tagged with the algorithmic bytes it moves.
 enum ProfKernel {
   PK_SPREAD = 0, PK_FFT_Z_FWD, PK_FFT_Y_FWD, PK_FFT_X_GREEN, PK_FFT_Y_INV, PK_FFT_Z_INV, PK_GATHER,
-  PK_PAIR_EF, PK_CSR_SPMV, PK_NEIGHBORS, PK_CG_VECTOR, PK_COUNT
+  PK_PAIR_EF, PK_CSR_SPMV, PK_NEIGHBORS, PK_CG_VECTOR,
+  // the CG matvec's mesh passes on the tensor cores
+  PK_TC_Z_FWD, PK_TC_Y_FWD, PK_TC_X, PK_TC_Y_INV, PK_TC_Z_INV, PK_COUNT
 };
 void count_launches(int n);
 bool prof_on();
